@@ -1,0 +1,235 @@
+/*
+ * cuopo.h -- C ABI of cuopo_b200, a B200 (sm_100a) split-step Fourier
+ * coupled-wave solver for optical parametric oscillators.
+ *
+ * The library is a drop-in for the crystal pass and the cavity round-trip
+ * loop of the reference simulator cuOPO.  Each entry point below names the
+ * reference interface it replaces (paths relative to the reference's
+ * repository root).  All functions return a cuopo_status and never exit
+ * the process.  Device pointers are plain CUDA device addresses; "stream"
+ * is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Field layout: one contiguous array of n_t interleaved complex values per
+ * field (re, im), float pairs for CUOPO_F32 plans and double pairs for
+ * CUOPO_F64 plans -- the layout of the reference's cufftComplex arrays.
+ */
+#ifndef CUOPO_H
+#define CUOPO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum {
+    CUOPO_OK = 0,
+    CUOPO_EINVAL = 1,       /* bad argument (sizes, pointers, ranges) */
+    CUOPO_ENOMEM = 2,       /* host or device allocation failed */
+    CUOPO_ECUDA = 3,        /* a CUDA runtime call failed */
+    CUOPO_ETIMEOUT = 4,     /* a bounded device-side wait gave up */
+    CUOPO_ENONFINITE = 5,   /* a field became NaN/Inf */
+    CUOPO_EUNSUPPORTED = 6, /* configuration not built into this library */
+    CUOPO_EIO = 7           /* file I/O failed */
+} cuopo_status;
+
+enum { CUOPO_PPLN = 0, CUOPO_SPPLT = 1 };   /* -DPPLN / -DSPPLT */
+enum { CUOPO_CW = 0, CUOPO_NS = 1 };        /* -DCW_OPO / -DNS_OPO */
+enum { CUOPO_F32 = 0, CUOPO_F64 = 1 };      /* field precision */
+
+/*
+ * Solver parameters: the arguments of EvolutionInCrystal
+ * (src/headers/cwes2.cuh:132, src/headers/cwes3.cuh:139) plus the values the
+ * round-trip loop src/cuOPO.cu:474-610 reads.  Units are the reference's:
+ * um, ps, V.  All values are doubles; the reference's own float values are
+ * represented exactly.
+ */
+typedef struct {
+    int n_eqs;          /* 2 or 3 (-DTHREE_EQS) */
+    int n_t;            /* grid points per round trip (SIZE), power of 2 */
+    int n_z;            /* slices per crystal pass (NZ) */
+    int regime;         /* CUOPO_CW or CUOPO_NS */
+    double vp, vs, vi;              /* group velocities [um/ps] */
+    double b2p, b2s, b2i;           /* GVD [ps^2/um] */
+    double b3p, b3s, b3i;           /* TOD [ps^3/um] */
+    double dk;                      /* phase mismatch [1/um] */
+    double kp, ks, ki;              /* coupling kappa [1/V] */
+    double dz;                      /* slice length [um] */
+    double alpha_crp, alpha_crs, alpha_cri;  /* absorption [1/um] */
+    double Rs, Ri;                  /* mirror reflectivities (fractions) */
+    double delta;                   /* detuning in units of pi */
+    double gdd;                     /* intracavity GDD [ps^2] */
+    double tod_s, tod_i;            /* TOD compensation [ps^3] */
+    int use_eom;                    /* intracavity phase modulator */
+    int eom_idler;                  /* modulator also acts on the idler */
+    double mod_depth;               /* modulation depth [rad] */
+    double fpm;                     /* modulation frequency [THz] */
+    double t_rt;                    /* round-trip time [ps] */
+    double ap0;                     /* CW pump amplitude [V/um] */
+} cuopo_params;
+
+/*
+ * Physical inputs: the reference's positional argv (src/cuOPO.sh:159,
+ * parsed at src/cuOPO.cu:92-267) plus the values it hard-codes, made
+ * run-time fields.  cuopo_inputs_default() fills the hard-coded values.
+ */
+typedef struct {
+    int crystal;            /* CUOPO_PPLN / CUOPO_SPPLT */
+    int n_eqs;              /* 2 or 3 */
+    int regime;             /* CUOPO_CW / CUOPO_NS */
+    int n_t;                /* SIZE (cuOPO.cu:28) */
+    int n_z;                /* NZ (cuOPO.cu:29) */
+    int n_rt;               /* NRT (cuOPO.cu:30) */
+    double lp_nm;           /* argv[1] pump wavelength [nm] */
+    double temp_c;          /* argv[2] (unused by the reference: T is scanned) */
+    double lambda_um;       /* argv[3] grating period [um] */
+    double n_thr;           /* argv[4] pump power / threshold */
+    double r_percent;       /* argv[5] signal reflectivity [%] */
+    double delta;           /* argv[6] detuning [units of pi] */
+    double gdd_percent;     /* argv[7] GDD compensation [% of crystal GDD] */
+    double tod_percent;     /* argv[8] TOD compensation [%] */
+    int use_eom;            /* argv[9] */
+    double mod_depth_pi;    /* argv[10] modulation depth [units of pi] */
+    double freq_det_mhz;    /* argv[11] EOM frequency detuning [MHz] */
+    double lcr_mm;          /* argv[12] crystal length [mm] */
+    double ls_nm;           /* signal wavelength; 0 = 2*lp (cuOPO.cu:93) */
+    int temp_from_scan;     /* 1 = scan 10..150 C like cuOPO.cu:100 */
+    double lcav_um;         /* cavity length (cuOPO.cu:129: 100e3) */
+    double ri;              /* idler reflectivity (cuOPO.cu:133: 0.98) */
+    double waist_um;        /* pump waist (cuOPO.cu:202: 55) */
+    double fwhm_ps;         /* NS pump FWHM (cuOPO.cu:244: 10000) */
+} cuopo_inputs;
+
+/* Derived quantities that the reference prints but the solver does not read. */
+typedef struct {
+    double temp_c, np, ns, ni, li, dkp, t_rt, fsr, finesse, ith, pth, power,
+        gamma_l, alphas, alphai, sigmap, dT, dF;
+} cuopo_info;
+
+/* ------------------------------------------------------------ host set-up */
+
+/* Fills the reference's hard-coded defaults (cuOPO.cu:28-30,93,129,133,202,244). */
+void cuopo_inputs_default(cuopo_inputs *in);
+
+/* Parameter derivation of src/cuOPO.cu:92-234 (Sellmeier: src/headers/ppln.cuh:33-189,
+ * src/headers/spplt.cuh:31-153; temperature scan: src/headers/functions.cuh:23-54),
+ * evaluated in float exactly as the reference does. */
+cuopo_status cuopo_derive_params(const cuopo_inputs *in, cuopo_params *out, cuopo_info *info);
+
+/* Sellmeier model of the crystal: which = 0 n, 1 dn/dl, 2 d2n/dl2, 3 d3n/dl3,
+ * 4 group velocity, 5 GVD, 6 TOD.  L in um, T in C.  (ppln.cuh:33-189) */
+float cuopo_sellmeier(int crystal, int which, float L, float T);
+
+/* findPhaseMatchingTemp, src/headers/functions.cuh:23-54. */
+float cuopo_phase_matching_temp(int crystal, float lp, float ls, float lambda_um,
+                                float t_min, float t_max);
+
+/* Grids of src/cuOPO.cu:169-189: T (n_t time points of one round trip) and
+ * w (angular frequency, fftshifted, with the reference's (n-1) linspace
+ * spacing).  Either output may be NULL. */
+cuopo_status cuopo_make_grids(int n_t, double t_rt, float *T, float *w);
+
+/* linspace (src/headers/functions.cuh:12-18) of length n into out. */
+void cuopo_linspace(float *out, long n, float xmin, float xmax);
+
+/* Pump inputs: CW constant (functions.cuh:91-100) and the NS Gaussian window
+ * over n_t*n_rt points (cuOPO.cu:164-175,243-248, functions.cuh:77-85). */
+cuopo_status cuopo_pump_cw(float *out_c32, int n_t, double ap0);
+cuopo_status cuopo_pump_ns(float *out_c32, int n_t, int n_rt, double t_rt,
+                           double ap0, double fwhm_ps);
+
+/* Seeded complex Gaussian noise (re and im each N(0, sigma^2)), replacing
+ * the clock-seeded NoiseGeneratorCPU (functions.cuh:58-71).  Philox4x32-10
+ * counter-based generator + Box-Muller; the host and device versions give
+ * identical bits.  out_c32 is float pairs (host or device pointer). */
+cuopo_status cuopo_noise_host(float *out_c32, long n, double sigma, uint64_t seed,
+                              uint64_t stream_id);
+cuopo_status cuopo_noise_device(void *out_c32, long n, double sigma, uint64_t seed,
+                                uint64_t stream_id, void *stream);
+
+/* .dat writers of src/headers/files.cuh:21-62: one value per line,
+ * 20 significant digits; complex vectors go to <name>_r.dat/<name>_i.dat. */
+cuopo_status cuopo_write_dat_real(const char *path, const float *v, long n);
+cuopo_status cuopo_write_dat_complex(const char *prefix, const float *v_c32, long n);
+/* Reader for the same format (n values expected). */
+cuopo_status cuopo_read_dat_complex(const char *prefix, float *v_c32, long n);
+
+/* ------------------------------------------------------------- GPU solver */
+
+typedef struct cuopo_plan cuopo_plan;
+
+/*
+ * Creates a plan: device-resident dispersion, GDD and RK4 tables for one
+ * parameter set, and the kernel configuration (cluster size, threads).
+ * w_host: the n_t angular frequencies the reference passes to
+ * EvolutionInCrystal as w_ext_gpu (cuOPO.cu:183-189); NULL = build them
+ * with cuopo_make_grids.  T_host likewise (used by the modulator).
+ * Replaces the set-up of cuOPO.cu:379-454 (buffers, cufftPlan1d).
+ */
+cuopo_status cuopo_plan_create(cuopo_plan **plan, const cuopo_params *p,
+                               const float *w_host, const float *T_host,
+                               int precision);
+cuopo_status cuopo_plan_destroy(cuopo_plan *plan);
+
+/* Cluster size and threads per CTA the plan launches with. */
+cuopo_status cuopo_plan_config(const cuopo_plan *plan, int *cluster, int *threads,
+                               int *smem_bytes);
+
+/*
+ * One crystal pass on device fields in place: EvolutionInCrystal,
+ * src/headers/cwes2.cuh:132-215 (n_eqs 2; Ai ignored) and
+ * src/headers/cwes3.cuh:139-225 (n_eqs 3).  One kernel launch.
+ */
+cuopo_status cuopo_crystal_pass(cuopo_plan *plan, void *Ap, void *As, void *Ai,
+                                void *stream);
+
+/*
+ * Round trips nn = rt_begin .. rt_begin+rt_count-1 of the loop body
+ * src/cuOPO.cu:474-610 on device fields in place, in one kernel launch:
+ * pump injection (CW copy of pump[0..n_t), :480; NS ReadPump of the
+ * n_t*n_rt window with its last-rt offset, :484), crystal pass, modulator
+ * (:509-518), GDD/TOD compensation (:521-553), AddPhase (:557-566),
+ * SaveRoundTrip (:570-608) of rts in [save_first, save_first+save_count)
+ * to slot nn-save_first of save_p/save_s/save_i (each n_t*save_count
+ * values; any may be NULL).  ps_hist (device, doubles, may be NULL) gets
+ * (1/n_t) sum|As|^2 after each rt.  If tol > 0 the launch stops after the
+ * first rt from the second on whose relative change of that power is
+ * below tol; *rt_done_dev (device int, may be NULL) gets the number of rts
+ * run.
+ */
+cuopo_status cuopo_round_trips(cuopo_plan *plan, void *Ap, void *As, void *Ai,
+                               const void *pump, int n_rt, int rt_begin, int rt_count,
+                               void *save_p, void *save_s, void *save_i,
+                               int save_first, int save_count,
+                               double *ps_hist, double tol, int *rt_done_dev,
+                               void *stream);
+
+/* Reads (and with reset != 0 clears) the plan's device-side status word:
+ * CUOPO_OK, or CUOPO_ENONFINITE if a launch met a NaN/Inf signal power
+ * (that instance stops at the round trip where it happened).  Synchronous. */
+cuopo_status cuopo_plan_status(cuopo_plan *plan, int *status, int reset);
+
+/* Blocks until the plan's work on stream has finished; returns the first
+ * asynchronous error. */
+cuopo_status cuopo_sync(void *stream);
+
+/* Text of the last error recorded by this thread (never NULL). */
+const char *cuopo_last_error(void);
+
+/* Library version string. */
+const char *cuopo_version(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUOPO_H */
