@@ -68,6 +68,12 @@ class Info(C.Structure):
         "gamma_l", "alphas", "alphai", "sigmap", "dT", "dF")]
 
 
+class Instance(C.Structure):
+    """cuopo_instance (include/cuopo.h)."""
+    _fields_ = [("n_t", C.c_int), ("ap0", C.c_double), ("Rs", C.c_double), ("delta", C.c_double),
+                ("gdd", C.c_double), ("seed", C.c_uint64)]
+
+
 _vp = C.c_void_p
 _fp = C.POINTER(C.c_float)
 _i = C.c_int
@@ -94,6 +100,15 @@ SIGNATURES = {
     "cuopo_crystal_pass": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cuopo_round_trips": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _i, _i, _vp, _d, _vp, _vp]),
     "cuopo_plan_status": (_i, [_vp, C.POINTER(_i), _i]),
+    "cuopo_fft_c2c": (_i, [_vp, _vp, _i, _i, _i, _i, _vp]),
+    "cuopo_batch_create": (_i, [C.POINTER(_vp), C.POINTER(Params), _vp, _i, _i]),
+    "cuopo_batch_destroy": (_i, [_vp]),
+    "cuopo_batch_total_elements": (_i, [_vp, C.POINTER(C.c_long)]),
+    "cuopo_batch_seed_noise": (_i, [_vp, _d, _vp]),
+    "cuopo_batch_set_signal": (_i, [_vp, _vp, _i, _vp]),
+    "cuopo_batch_get_signal": (_i, [_vp, _vp, _i, _vp]),
+    "cuopo_batch_run": (_i, [_vp, _i, _d, _i, _vp]),
+    "cuopo_batch_results": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

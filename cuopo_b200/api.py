@@ -193,5 +193,82 @@ class Plan:
             _ptr(rt_done), _stream(stream)))
 
 
+def fft_c2c(x, sign: int, out=None, stream=None):
+    """Batched unnormalised C2C FFT over the last axis of a CUDA tensor
+    (sign +1 = CUFFT_INVERSE, -1 = CUFFT_FORWARD); the cufftExecC2C stand-in."""
+    import torch
+    assert x.is_cuda and x.is_contiguous() and x.dtype in (torch.complex64, torch.complex128)
+    out = torch.empty_like(x) if out is None else out
+    n = x.shape[-1]
+    prec = F32 if x.dtype == torch.complex64 else F64
+    check(load().cuopo_fft_c2c(x.data_ptr(), out.data_ptr(), n, x.numel() // n, sign, prec, _stream(stream)))
+    return out
+
+
 def sync(stream=None) -> None:
     check(load().cuopo_sync(_stream(stream) if stream is not None else None))
+
+
+class Batch:
+    """A batched CW sweep (cuopo_batch_*): many instances, one persistent launch per grid size."""
+
+    def __init__(self, base: Params, instances, precision: int = F32):
+        from ._lib import Instance
+        self._lib = load()
+        arr = (Instance * len(instances))()
+        for k, inst in enumerate(instances):
+            for name, val in inst.items():
+                setattr(arr[k], name, val)
+        self.count = len(instances)
+        self.n_t = np.array([i["n_t"] for i in instances])
+        self.precision = precision
+        h = C.c_void_p()
+        check(self._lib.cuopo_batch_create(C.byref(h), C.byref(base), arr, len(instances), precision))
+        self._h = h
+        n = C.c_long()
+        check(self._lib.cuopo_batch_total_elements(self._h, C.byref(n)))
+        self.total = n.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.cuopo_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def seed_noise(self, sigma: float, stream=None) -> None:
+        check(self._lib.cuopo_batch_seed_noise(self._h, sigma, _stream(stream)))
+
+    def set_signal(self, src, stream=None) -> None:
+        """src: CUDA tensor or host numpy array with the concatenated signals."""
+        if isinstance(src, np.ndarray):
+            check(self._lib.cuopo_batch_set_signal(self._h, src.ctypes.data, 0, _stream(stream)))
+        else:
+            check(self._lib.cuopo_batch_set_signal(self._h, src.data_ptr(), int(src.is_cuda), _stream(stream)))
+
+    def get_signal(self, dst, stream=None) -> None:
+        if isinstance(dst, np.ndarray):
+            check(self._lib.cuopo_batch_get_signal(self._h, dst.ctypes.data, 0, _stream(stream)))
+        else:
+            check(self._lib.cuopo_batch_get_signal(self._h, dst.data_ptr(), int(dst.is_cuda), _stream(stream)))
+
+    def run(self, max_rt: int, tol: float, patience: int = 1, stream=None) -> None:
+        check(self._lib.cuopo_batch_run(self._h, max_rt, tol, patience, _stream(stream)))
+
+    def results(self, stream=None):
+        ps = np.zeros(self.count)
+        rts = np.zeros(self.count, np.int32)
+        flags = np.zeros(self.count, np.int32)
+        check(self._lib.cuopo_batch_results(self._h, ps.ctypes.data, rts.ctypes.data, flags.ctypes.data,
+                                            _stream(stream)))
+        return ps, rts, flags

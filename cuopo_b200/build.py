@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CC_FLAGS = ["-O2", "-fPIC", "-std=c11", "-Wall", "-Wextra", "-fvisibility=hidden", "-I" + str(INCLUDE),
             "-I" + str(CSRC)]
 
-CU_SOURCES = ["solver.cu", "noise.cu"]
+CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu"]
 C_SOURCES = ["params.c", "dat_io.c"]
 
 
@@ -84,7 +84,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         list(ex.map(lambda c: _run(c, verbose or ptxas_verbose), jobs))
     if force or jobs or not LIB.exists():
         tmp = LIB.with_suffix(".so.tmp")
-        _run([_nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-lm"], verbose)
+        _run([_nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", str(tmp), *map(str, objs), "-lm"], verbose)
         os.replace(tmp, LIB)
     return LIB
 

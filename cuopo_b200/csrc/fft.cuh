@@ -17,9 +17,14 @@
  * those registers with no shared-memory exchange or barrier.
  *
  * Twiddles: a radix-16 stage whose sub-transform length is NS needs
- * W^{r k}, W = exp(2 pi i/(16 NS)), k = t mod NS, r = 1..15.  The base W^k
- * is formed once per thread in double precision (sincospi); its powers
- * are built by products of depth <= 4 from it.
+ * W^{r k}, W = exp(2 pi i/(16 NS)), k = t mod NS, r = 1..15, fixed per
+ * thread for the whole kernel.  Middle stages (NS <= M/256) read them from
+ * a small shared-memory table formed in FP64 when the kernel starts
+ * (15 NS entries per stage); the last stage (NS = M/16, one set per
+ * thread) keeps the six FP64-rounded powers W^{k}, W^{2k}, W^{3k}, W^{4k},
+ * W^{8k}, W^{12k} in registers and forms the others as one product
+ * W^{4a k} W^{b k}.  Every twiddle is therefore within two roundings of
+ * exact.
  */
 #pragma once
 #include "cplx.cuh"
@@ -130,33 +135,6 @@ __device__ __forceinline__ void dft(C (&v)[RADIX])
     else dft16<S>(v);
 }
 
-/* v[r] *= w^r, r = 1..15, w = base (S=+1 form) or its conjugate. */
-template <int S, typename C>
-__device__ __forceinline__ void apply_twiddles16(C (&v)[16], C base)
-{
-    const C w1 = S > 0 ? base : cconj(base);
-    const C w2 = cmul(w1, w1);
-    const C w3 = cmul(w2, w1);
-    const C w4 = cmul(w2, w2);
-    const C w8 = cmul(w4, w4);
-    const C w12 = cmul(w8, w4);
-    v[1] = cmul(v[1], w1);
-    v[2] = cmul(v[2], w2);
-    v[3] = cmul(v[3], w3);
-    v[4] = cmul(v[4], w4);
-    v[5] = cmul(cmul(v[5], w4), w1);
-    v[6] = cmul(cmul(v[6], w4), w2);
-    v[7] = cmul(cmul(v[7], w4), w3);
-    v[8] = cmul(v[8], w8);
-    v[9] = cmul(cmul(v[9], w8), w1);
-    v[10] = cmul(cmul(v[10], w8), w2);
-    v[11] = cmul(cmul(v[11], w8), w3);
-    v[12] = cmul(v[12], w12);
-    v[13] = cmul(cmul(v[13], w12), w1);
-    v[14] = cmul(cmul(v[14], w12), w2);
-    v[15] = cmul(cmul(v[15], w12), w3);
-}
-
 /* Shared-memory index swizzle: XOR of the low bits with the row number so
  * that the stride-R stores of early stages hit distinct banks.  Rows are
  * 128 bytes (16 float2 or 8 double2). */
@@ -185,26 +163,99 @@ struct StagePlan {
     }
 };
 
-/* Per-thread twiddle bases W^{t mod NS_p} of the radix-16 stages p >= 1
- * (S = +1 form), formed in double precision. */
+/* Shared-memory twiddle table of the middle radix-16 stages 1..P-2:
+ * entry (p, r, k) = W_{16 NS_p}^{r k}, r = 1..15, k < NS_p. */
+template <int M>
+struct TwTable {
+    using SP = StagePlan<M>;
+    static constexpr int offset(int p)
+    {
+        int o = 0;
+        for (int q = 1; q < p; q++) o += 15 * SP::ns(q);
+        return o;
+    }
+    static constexpr int size() { return SP::P > 2 ? offset(SP::P - 1) : 0; }
+};
+
+/* Fills the table (all threads of the CTA cooperate; caller syncs). */
+template <int M, typename C>
+__device__ __forceinline__ void fill_twiddle_table(C *tab, int t)
+{
+    using SP = StagePlan<M>;
+    using R = typename real_of<C>::type;
+#pragma unroll
+    for (int p = 1; p + 1 < SP::P; p++) {
+        const int ns = SP::ns(p);
+        const int off = TwTable<M>::offset(p);
+        for (int idx = t; idx < 15 * ns; idx += SP::T) {
+            const int r = idx / ns + 1, k = idx % ns;
+            double sn, cs;
+            sincospi(2.0 * (double)(r * k) / (16.0 * (double)ns), &sn, &cs);
+            tab[off + idx] = mk<C>((R)cs, (R)sn);
+        }
+    }
+}
+
+/* The last radix-16 stage's twiddles of thread t (S = +1 form). */
 template <int M, typename C>
 struct StageTwiddles {
-    static constexpr int P = StagePlan<M>::P;
-    static constexpr int NT = P > 1 ? P - 1 : 1;
-    C w[NT];
-    __device__ __forceinline__ void init(int t)
+    C w1, w2, w3, w4, w8, w12;
+    const C *tab;  /* shared-memory table of the middle stages */
+    __device__ __forceinline__ void init(int t, const C *table)
     {
         using R = typename real_of<C>::type;
-#pragma unroll
-        for (int p = 1; p < P; p++) {
-            const int ns = StagePlan<M>::ns(p);
-            const int k = t % ns;
-            double s, c;
-            sincospi(2.0 * (double)k / (16.0 * (double)ns), &s, &c);
-            w[p - 1] = mk<C>((R)c, (R)s);
+        using SP = StagePlan<M>;
+        tab = table;
+        if constexpr (SP::P > 1) {
+            const int ns = SP::ns(SP::P - 1);
+            const double k = (double)(t % ns);
+            const double den = 16.0 * (double)ns;
+            double sn, cs;
+            sincospi(2.0 * k / den, &sn, &cs);
+            w1 = mk<C>((R)cs, (R)sn);
+            sincospi(4.0 * k / den, &sn, &cs);
+            w2 = mk<C>((R)cs, (R)sn);
+            sincospi(6.0 * k / den, &sn, &cs);
+            w3 = mk<C>((R)cs, (R)sn);
+            sincospi(8.0 * k / den, &sn, &cs);
+            w4 = mk<C>((R)cs, (R)sn);
+            sincospi(16.0 * k / den, &sn, &cs);
+            w8 = mk<C>((R)cs, (R)sn);
+            sincospi(24.0 * k / den, &sn, &cs);
+            w12 = mk<C>((R)cs, (R)sn);
         }
     }
 };
+
+template <int S, typename C>
+__device__ __forceinline__ C cj(C a)
+{
+    return S > 0 ? a : cconj(a);
+}
+
+/* v[4a+b] *= W^{(4a+b)k} from the six register powers (last stage). */
+template <int S, typename C>
+__device__ __forceinline__ void apply_last_twiddles(C (&v)[16], const C &w1, const C &w2, const C &w3,
+                                                    const C &w4, const C &w8, const C &w12)
+{
+    const C b1 = cj<S>(w1), b2 = cj<S>(w2), b3 = cj<S>(w3);
+    const C a1 = cj<S>(w4), a2 = cj<S>(w8), a3 = cj<S>(w12);
+    v[1] = cmul(v[1], b1);
+    v[2] = cmul(v[2], b2);
+    v[3] = cmul(v[3], b3);
+    v[4] = cmul(v[4], a1);
+    v[5] = cmul(v[5], cmul(a1, b1));
+    v[6] = cmul(v[6], cmul(a1, b2));
+    v[7] = cmul(v[7], cmul(a1, b3));
+    v[8] = cmul(v[8], a2);
+    v[9] = cmul(v[9], cmul(a2, b1));
+    v[10] = cmul(v[10], cmul(a2, b2));
+    v[11] = cmul(v[11], cmul(a2, b3));
+    v[12] = cmul(v[12], a3);
+    v[13] = cmul(v[13], cmul(a3, b1));
+    v[14] = cmul(v[14], cmul(a3, b2));
+    v[15] = cmul(v[15], cmul(a3, b3));
+}
 
 template <int S, int M, int P_IDX, typename C>
 __device__ __forceinline__ void stage_compute(C (&reg)[16], const StageTwiddles<M, C> &tw)
@@ -220,7 +271,14 @@ __device__ __forceinline__ void stage_compute(C (&reg)[16], const StageTwiddles<
         for (int r = 0; r < R; r++) v[r] = reg[b + r * B];
         if constexpr (NS > 1) {
             static_assert(R == 16, "twiddled stages are radix 16");
-            apply_twiddles16<S>(v, tw.w[P_IDX - 1]);
+            if constexpr (P_IDX + 1 == SP::P) {
+                apply_last_twiddles<S>(v, tw.w1, tw.w2, tw.w3, tw.w4, tw.w8, tw.w12);
+            } else {
+                const int k = threadIdx.x % NS;
+                const C *row = tw.tab + TwTable<M>::offset(P_IDX) + k;
+#pragma unroll
+                for (int r = 1; r < 16; r++) v[r] = cmul(v[r], cj<S>(row[(r - 1) * NS]));
+            }
         }
         dft<S, R>(v);
 #pragma unroll

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "cuopo.h"
@@ -55,21 +56,39 @@ extern "C" const char *cuopo_version(void) { return "cuopo_b200 0.1.0 (sm_100a)"
 /* -------------------------------------------------------- kernel registry */
 
 typedef cudaError_t (*launch_fn)(const LaunchArgs &, int grid, cudaStream_t);
+typedef int (*occ_fn)(void);
 
-template <typename R, int F, int M, bool INPLACE>
+template <typename R, int F, int M, bool INPLACE, int MINB>
+static cudaError_t prepare_kernel()
+{
+    using K = Ssfm<R, F, M, INPLACE>;
+    static cudaError_t st = cudaFuncSetAttribute(ssfm_kernel<R, F, M, INPLACE, MINB>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)K::smem_bytes());
+    return st;
+}
+
+template <typename R, int F, int M, bool INPLACE, int MINB>
 static cudaError_t launch_impl(const LaunchArgs &a, int grid, cudaStream_t st)
 {
     using K = Ssfm<R, F, M, INPLACE>;
-    const size_t smem = K::smem_bytes();
-    static bool attr_done = false;  /* per-instantiation, set on first use */
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, INPLACE>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_done = true;
-    }
-    ssfm_kernel<R, F, M, INPLACE><<<grid, K::T, smem, st>>>(a);
+    cudaError_t e = prepare_kernel<R, F, M, INPLACE, MINB>();
+    if (e != cudaSuccess) return e;
+    ssfm_kernel<R, F, M, INPLACE, MINB><<<grid, K::T, K::smem_bytes(), st>>>(a);
     return cudaGetLastError();
+}
+
+/* Resident CTAs per SM of this kernel (0 on error). */
+template <typename R, int F, int M, bool INPLACE, int MINB>
+static int occupancy_impl()
+{
+    using K = Ssfm<R, F, M, INPLACE>;
+    if (prepare_kernel<R, F, M, INPLACE, MINB>() != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ssfm_kernel<R, F, M, INPLACE, MINB>, K::T,
+                                                      K::smem_bytes()) != cudaSuccess)
+        return 0;
+    return n;
 }
 
 struct KernelEntry {
@@ -77,30 +96,32 @@ struct KernelEntry {
     bool inplace;
     size_t smem;
     launch_fn fn;
+    occ_fn occ;
 };
 
-#define CUOPO_K(R, PREC, F, M, IP) \
-    {PREC, F, M, IP, Ssfm<R, F, M, IP>::smem_bytes(), &launch_impl<R, F, M, IP>}
+#define CUOPO_K(R, PREC, F, M, IP, MINB)                                             \
+    {PREC, F, M, IP, Ssfm<R, F, M, IP>::smem_bytes(), &launch_impl<R, F, M, IP, MINB>, \
+     &occupancy_impl<R, F, M, IP, MINB>}
 
 static const KernelEntry k_kernels[] = {
-    CUOPO_K(float, CUOPO_F32, 2, 512, false),
-    CUOPO_K(float, CUOPO_F32, 2, 1024, false),
-    CUOPO_K(float, CUOPO_F32, 2, 2048, false),
-    CUOPO_K(float, CUOPO_F32, 2, 4096, false),
-    CUOPO_K(float, CUOPO_F32, 2, 8192, false),
-    CUOPO_K(float, CUOPO_F32, 3, 512, false),
-    CUOPO_K(float, CUOPO_F32, 3, 1024, false),
-    CUOPO_K(float, CUOPO_F32, 3, 2048, false),
-    CUOPO_K(float, CUOPO_F32, 3, 4096, false),
-    CUOPO_K(float, CUOPO_F32, 3, 8192, true),
-    CUOPO_K(double, CUOPO_F64, 2, 512, false),
-    CUOPO_K(double, CUOPO_F64, 2, 1024, false),
-    CUOPO_K(double, CUOPO_F64, 2, 2048, false),
-    CUOPO_K(double, CUOPO_F64, 2, 4096, false),
-    CUOPO_K(double, CUOPO_F64, 3, 512, false),
-    CUOPO_K(double, CUOPO_F64, 3, 1024, false),
-    CUOPO_K(double, CUOPO_F64, 3, 2048, false),
-    CUOPO_K(double, CUOPO_F64, 3, 4096, true),
+    CUOPO_K(float, CUOPO_F32, 2, 512, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 1024, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 2048, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 4096, false, 2),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 512, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 1024, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 2048, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 4096, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 8192, true, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 512, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 1024, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 2048, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 512, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 1024, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 2048, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 4096, true, 1),
 };
 
 static const KernelEntry *find_kernel(int precision, int F, int N)
@@ -402,5 +423,259 @@ extern "C" cuopo_status cuopo_sync(void *stream)
 {
     cudaError_t e = stream ? cudaStreamSynchronize((cudaStream_t)stream) : cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "sync");
+    return CUOPO_OK;
+}
+
+/* ------------------------------------------------------------------ batches */
+
+struct BatchGroup {
+    int n_t;
+    cuopo_plan *plan;
+    std::vector<int> members;
+    Instance *d_inst;
+    int *d_queue;
+    cudaStream_t stream;
+    cudaEvent_t done;
+    int grid;
+};
+
+struct cuopo_batch {
+    int count;
+    int precision;
+    int F;
+    cuopo_params base;
+    std::vector<cuopo_instance> inst;
+    std::vector<size_t> offset;   /* element offset of each instance's signal */
+    size_t total;                 /* total signal elements */
+    void *d_pump;                 /* pump-field work buffers (n_t per instance) */
+    void *d_signal;               /* signal fields, concatenated */
+    double *d_ps;
+    int *d_rt;
+    int *d_flag;
+    std::vector<BatchGroup> groups;
+    cudaEvent_t fork;
+    std::vector<Instance> h_inst;
+};
+
+extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
+{
+    if (!b) return CUOPO_OK;
+    for (BatchGroup &g : b->groups) {
+        cuopo_plan_destroy(g.plan);
+        cudaFree(g.d_inst);
+        cudaFree(g.d_queue);
+        if (g.stream) cudaStreamDestroy(g.stream);
+        if (g.done) cudaEventDestroy(g.done);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    cudaFree(b->d_pump);
+    cudaFree(b->d_signal);
+    cudaFree(b->d_ps);
+    cudaFree(b->d_rt);
+    cudaFree(b->d_flag);
+    delete b;
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params *base, const cuopo_instance *inst,
+                                           int count, int precision)
+{
+    if (!out || !base || !inst || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create: bad argument");
+    *out = nullptr;
+    if (base->n_eqs != 2) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW 2-equation sweeps");
+    if (base->regime != CUOPO_CW) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW sweeps");
+    if (precision != CUOPO_F32 && precision != CUOPO_F64)
+        return cuopo_fail(CUOPO_EINVAL, "batch_create: bad precision");
+    for (int i = 0; i < count; i++) {
+        if (!is_pow2i(inst[i].n_t) || !find_kernel(precision, 2, inst[i].n_t))
+            return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: an instance has an unsupported n_t");
+        if (!(inst[i].Rs >= 0.0 && inst[i].Rs <= 1.0)) return cuopo_fail(CUOPO_EINVAL, "batch_create: Rs out of [0,1]");
+    }
+    cuopo_batch *b = new (std::nothrow) cuopo_batch();
+    if (!b) return cuopo_fail(CUOPO_ENOMEM, "batch_create: out of host memory");
+    b->count = count;
+    b->precision = precision;
+    b->F = 2;
+    b->base = *base;
+    b->inst.assign(inst, inst + count);
+    b->offset.resize(count);
+    size_t off = 0;
+    for (int i = 0; i < count; i++) {
+        b->offset[i] = off;
+        off += (size_t)inst[i].n_t;
+    }
+    b->total = off;
+    const size_t esz = precision == CUOPO_F32 ? 8 : 16;
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_pump, esz * off)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_signal, esz * off)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_ps, sizeof(double) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_rt, sizeof(int) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_flag, sizeof(int) * count)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) {
+        cuopo_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? cuopo_fail(CUOPO_ENOMEM, "batch_create: device allocation failed")
+                                              : cuda_fail(e, "batch_create");
+    }
+    cudaMemset(b->d_pump, 0, esz * off);
+    cudaMemset(b->d_signal, 0, esz * off);
+    cudaMemset(b->d_ps, 0, sizeof(double) * count);
+    cudaMemset(b->d_rt, 0, sizeof(int) * count);
+    cudaMemset(b->d_flag, 0, sizeof(int) * count);
+
+    /* one plan (tables) and one persistent launch per distinct grid size */
+    std::vector<int> sizes;
+    for (int i = 0; i < count; i++)
+        if (std::find(sizes.begin(), sizes.end(), inst[i].n_t) == sizes.end()) sizes.push_back(inst[i].n_t);
+    std::sort(sizes.begin(), sizes.end(), [](int a, int c) { return a > c; });
+    b->h_inst.resize(count);
+    for (int n_t : sizes) {
+        BatchGroup g{};
+        g.n_t = n_t;
+        cuopo_params p = *base;
+        p.n_t = n_t;
+        cuopo_status st = cuopo_plan_create(&g.plan, &p, nullptr, nullptr, precision);
+        if (st != CUOPO_OK) {
+            cuopo_batch_destroy(b);
+            return st;
+        }
+        for (int i = 0; i < count; i++)
+            if (inst[i].n_t == n_t) g.members.push_back(i);
+        const KernelEntry *k = find_kernel(precision, 2, n_t);
+        int occ = k->occ();
+        if (occ < 1) {
+            b->groups.push_back(g);
+            cuopo_batch_destroy(b);
+            return cuopo_fail(CUOPO_ECUDA, "batch_create: kernel does not fit on an SM");
+        }
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g.grid = std::min((int)g.members.size(), occ * sms);
+        if ((e = cudaMalloc(&g.d_inst, sizeof(Instance) * g.members.size())) != cudaSuccess ||
+            (e = cudaMalloc(&g.d_queue, sizeof(int))) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming)) != cudaSuccess) {
+            b->groups.push_back(g);
+            cuopo_batch_destroy(b);
+            return cuda_fail(e, "batch_create");
+        }
+        std::vector<Instance> hi(g.members.size());
+        for (size_t j = 0; j < g.members.size(); j++) {
+            const int i = g.members[j];
+            Instance &I = hi[j];
+            std::memset(&I, 0, sizeof(I));
+            I.Ap = (char *)b->d_pump + esz * b->offset[i];
+            I.As = (char *)b->d_signal + esz * b->offset[i];
+            I.Ai = nullptr;
+            I.pump = nullptr;
+            I.ap0 = inst[i].ap0;
+            cuopo_params pi = p;
+            pi.Rs = inst[i].Rs;
+            pi.delta = inst[i].delta;
+            pi.gdd = inst[i].gdd;
+            cavity_factors(pi, I);
+            I.ps_out = b->d_ps + i;
+            I.rt_done = b->d_rt + i;
+            I.flag_out = b->d_flag + i;
+            b->h_inst[i] = I;
+        }
+        if ((e = cudaMemcpy(g.d_inst, hi.data(), sizeof(Instance) * hi.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            b->groups.push_back(g);
+            cuopo_batch_destroy(b);
+            return cuda_fail(e, "batch_create: upload");
+        }
+        b->groups.push_back(g);
+    }
+    *out = b;
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_total_elements(const cuopo_batch *b, long *n)
+{
+    if (!b || !n) return cuopo_fail(CUOPO_EINVAL, "batch_total_elements: NULL argument");
+    *n = (long)b->total;
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_seed_noise(cuopo_batch *b, double sigma, void *stream)
+{
+    if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_seed_noise: NULL batch");
+    if (b->precision != CUOPO_F32) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_seed_noise: F32 batches only");
+    for (int i = 0; i < b->count; i++) {
+        cuopo_status st = cuopo_noise_device((char *)b->d_signal + 8 * b->offset[i], b->inst[i].n_t, sigma,
+                                             b->inst[i].seed, 0, stream);
+        if (st != CUOPO_OK) return st;
+    }
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_set_signal(cuopo_batch *b, const void *src, int on_device, void *stream)
+{
+    if (!b || !src) return cuopo_fail(CUOPO_EINVAL, "batch_set_signal: NULL argument");
+    const size_t esz = b->precision == CUOPO_F32 ? 8 : 16;
+    cudaError_t e = cudaMemcpyAsync(b->d_signal, src, esz * b->total,
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    (cudaStream_t)stream);
+    return e == cudaSuccess ? CUOPO_OK : cuda_fail(e, "batch_set_signal");
+}
+
+extern "C" cuopo_status cuopo_batch_get_signal(cuopo_batch *b, void *dst, int on_device, void *stream)
+{
+    if (!b || !dst) return cuopo_fail(CUOPO_EINVAL, "batch_get_signal: NULL argument");
+    const size_t esz = b->precision == CUOPO_F32 ? 8 : 16;
+    cudaError_t e = cudaMemcpyAsync(dst, b->d_signal, esz * b->total,
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    (cudaStream_t)stream);
+    return e == cudaSuccess ? CUOPO_OK : cuda_fail(e, "batch_get_signal");
+}
+
+extern "C" cuopo_status cuopo_batch_run(cuopo_batch *b, int max_rt, double tol, int patience, void *stream)
+{
+    if (!b || max_rt < 1) return cuopo_fail(CUOPO_EINVAL, "batch_run: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaEventRecord(b->fork, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch_run");
+    for (BatchGroup &g : b->groups) {
+        if ((e = cudaStreamWaitEvent(g.stream, b->fork, 0)) != cudaSuccess) return cuda_fail(e, "batch_run");
+        if ((e = cudaMemsetAsync(g.d_queue, 0, sizeof(int), g.stream)) != cudaSuccess) return cuda_fail(e, "batch_run");
+        LaunchArgs a = base_args(g.plan);
+        a.inst = g.d_inst;
+        a.n_inst = (int)g.members.size();
+        a.queue = g.d_queue;
+        /* rt window, tolerance and patience are per run: patch the descriptors */
+        std::vector<Instance> hi(g.members.size());
+        for (size_t j = 0; j < g.members.size(); j++) {
+            hi[j] = b->h_inst[g.members[j]];
+            hi[j].rt_begin = 0;
+            hi[j].rt_count = max_rt;
+            hi[j].tol = tol;
+            hi[j].patience = patience;
+        }
+        if ((e = cudaMemcpyAsync(g.d_inst, hi.data(), sizeof(Instance) * hi.size(), cudaMemcpyHostToDevice,
+                                 g.stream)) != cudaSuccess)
+            return cuda_fail(e, "batch_run: upload");
+        /* the pageable copy above is staged before the call returns */
+        cuopo_status s2 = launch(g.plan, a, g.grid, g.stream);
+        if (s2 != CUOPO_OK) return s2;
+        if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess) return cuda_fail(e, "batch_run");
+        if ((e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess) return cuda_fail(e, "batch_run");
+    }
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_results(cuopo_batch *b, double *ps, int *rts, int *flags, void *stream)
+{
+    if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_results: NULL batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (ps && (e = cudaMemcpyAsync(ps, b->d_ps, sizeof(double) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "batch_results");
+    if (rts && (e = cudaMemcpyAsync(rts, b->d_rt, sizeof(int) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "batch_results");
+    if (flags &&
+        (e = cudaMemcpyAsync(flags, b->d_flag, sizeof(int) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "batch_results");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch_results");
     return CUOPO_OK;
 }

@@ -57,6 +57,9 @@ struct Instance {
     double gdd;                 /* intracavity GDD [ps^2]; 0 = off */
     double tod_s, tod_i;        /* TOD compensation [ps^3] */
     int use_tod_s, use_tod_i;
+    int patience;               /* consecutive rts below tol to stop (>= 1) */
+    double *ps_out;             /* final signal power (may be NULL) */
+    int *flag_out;              /* 1 converged, 0 max rts reached, 5 non-finite (may be NULL) */
 };
 
 struct LaunchArgs {
@@ -125,8 +128,10 @@ struct Ssfm {
     static constexpr int P = SP::P;
     static constexpr int NCO = (F == 2) ? 6 : 3;
 
-    /* Shared memory: home[F][M] (+ scratch[M]) complex values. */
-    static constexpr size_t smem_bytes() { return sizeof(C) * (size_t)M * (F + (INPLACE ? 0 : 1)); }
+    /* Shared memory: home[F][M] (+ scratch[M]) complex values, then the
+     * twiddle table of the middle FFT stages. */
+    static constexpr size_t field_elems() { return (size_t)M * (F + (INPLACE ? 0 : 1)); }
+    static constexpr size_t smem_bytes() { return sizeof(C) * (field_elems() + TwTable<M>::size()); }
 
     /* T->W, multiply by the table row (or the on-the-fly GDD factor),
      * W->T, on the field at home. */
@@ -182,8 +187,11 @@ struct Ssfm {
         __shared__ int next_inst;
         const int t = threadIdx.x;
 
+        C *twtab = home + field_elems();
+        fill_twiddle_table<M>(twtab, t);
         StageTwiddles<M, C> tw;
-        tw.init(t);
+        tw.init(t, twtab);
+        __syncthreads();
         const R h6 = (R)a.tab.h6;
         const C *__restrict__ rk = reinterpret_cast<const C *>(a.tab.rk);
         const C *__restrict__ disp = reinterpret_cast<const C *>(a.tab.disp);
@@ -213,8 +221,8 @@ struct Ssfm {
 #pragma unroll
                 for (int e = 0; e < 16; e++) home[f * M + swz<C>(t + e * T)] = gf[f][t + e * T];
 
-            double prev_ps = -1.0;
-            int rts = 0;
+            double prev_ps = -1.0, ps = 0.0;
+            int rts = 0, calm = 0, flag = 0;
             bool stop = false;
             for (int rt = I.rt_begin; rt < I.rt_begin + I.rt_count && !stop; rt++) {
                 /* pump injection + first half step of slice 0 */
@@ -313,29 +321,42 @@ struct Ssfm {
                     }
                     acc += cabs2d(A[1]);
                 }
-                const double ps = block_sum(acc, red, t) * a.tab.inv_n;
+                ps = block_sum(acc, red, t) * a.tab.inv_n;
                 if (t == 0 && I.ps_hist) I.ps_hist[rt - I.rt_begin] = ps;
                 if (!(ps == ps) || ps > 1.0e300) {
                     if (t == 0 && a.status) atomicCAS(a.status, 0, (int)ST_NONFINITE);
+                    flag = ST_NONFINITE;
                     stop = true;
                 }
-                if (I.tol > 0.0 && prev_ps > 0.0 && ps > 0.0 && fabs(ps - prev_ps) < I.tol * ps)
-                    stop = true;
+                /* convergence: relative change of the signal power per rt below
+                 * tol for `patience` consecutive rts (from the second rt on) */
+                if (I.tol > 0.0 && prev_ps > 0.0 && ps > 0.0 && fabs(ps - prev_ps) < I.tol * ps) {
+                    if (++calm >= (I.patience > 0 ? I.patience : 1) && flag == 0) {
+                        flag = 1;
+                        stop = true;
+                    }
+                } else {
+                    calm = 0;
+                }
                 prev_ps = ps;
             }
 #pragma unroll
             for (int f = 0; f < F; f++)
 #pragma unroll
                 for (int e = 0; e < 16; e++) gf[f][t + e * T] = home[f * M + swz<C>(t + e * T)];
-            if (t == 0 && I.rt_done) *I.rt_done = rts;
+            if (t == 0) {
+                if (I.rt_done) *I.rt_done = rts;
+                if (I.ps_out) *I.ps_out = ps;
+                if (I.flag_out) *I.flag_out = flag;
+            }
             __syncthreads();
             if (!a.inst) break;
         }
     }
 };
 
-template <typename R, int F, int M, bool INPLACE>
-__global__ void __launch_bounds__(M / 16) ssfm_kernel(const LaunchArgs a)
+template <typename R, int F, int M, bool INPLACE, int MINB>
+__global__ void __launch_bounds__(M / 16, MINB) ssfm_kernel(const LaunchArgs a)
 {
     Ssfm<R, F, M, INPLACE>::run(a);
 }

@@ -214,6 +214,57 @@ cuopo_status cuopo_round_trips(cuopo_plan *plan, void *Ap, void *As, void *Ai,
  * (that instance stops at the round trip where it happened).  Synchronous. */
 cuopo_status cuopo_plan_status(cuopo_plan *plan, int *status, int reset);
 
+/*
+ * The library's FFT alone: `batch` unnormalised C2C transforms of n points
+ * (in place when in == out), exponent sign +1 = CUFFT_INVERSE, -1 =
+ * CUFFT_FORWARD.  Replaces cufftPlan1d/cufftExecC2C of the reference
+ * (src/headers/cwes2.cuh:139-140,170-182; src/cuOPO.cu:453-454,522-550).
+ * n: power of 2 in [512, 8192] (F32) or [512, 4096] (F64).
+ */
+cuopo_status cuopo_fft_c2c(const void *in, void *out, int n, int batch, int sign,
+                           int precision, void *stream);
+
+/* ------------------------------------------------------- batched sweeps */
+
+/*
+ * One point of a CW 2-equation parameter sweep.  The reference runs every
+ * sweep point as its own process (the nested loops of src/cuOPO.sh:91-174
+ * around ./cuOPO); a batch runs them all in one persistent launch per
+ * distinct grid size, every instance in its own CTA with its fields in
+ * shared memory, until it converges or reaches the round-trip limit.
+ */
+typedef struct {
+    int n_t;            /* grid points of this instance (power of 2) */
+    double ap0;         /* CW pump amplitude [V/um] (cuOPO.cu:229) */
+    double Rs;          /* signal mirror reflectivity, fraction (cuOPO.cu:130) */
+    double delta;       /* detuning in units of pi (cuOPO.cu:140) */
+    double gdd;         /* intracavity GDD [ps^2] (cuOPO.cu:142) */
+    uint64_t seed;      /* seed of the initial signal noise */
+} cuopo_instance;
+
+typedef struct cuopo_batch cuopo_batch;
+
+/* base supplies the crystal and everything not in cuopo_instance. */
+cuopo_status cuopo_batch_create(cuopo_batch **batch, const cuopo_params *base,
+                                const cuopo_instance *inst, int count, int precision);
+cuopo_status cuopo_batch_destroy(cuopo_batch *batch);
+/* Number of signal values of all instances (sum of n_t). */
+cuopo_status cuopo_batch_total_elements(const cuopo_batch *batch, long *n);
+/* Signal of every instance := seeded noise (cuopo_noise_device with the
+ * instance's seed, stream id 0). */
+cuopo_status cuopo_batch_seed_noise(cuopo_batch *batch, double sigma, void *stream);
+/* Copies all signals in/out: instances concatenated in creation order. */
+cuopo_status cuopo_batch_set_signal(cuopo_batch *batch, const void *src, int src_on_device, void *stream);
+cuopo_status cuopo_batch_get_signal(cuopo_batch *batch, void *dst, int dst_on_device, void *stream);
+/* Runs every instance from round trip 0 until the relative change of its
+ * signal power per round trip stays below tol for `patience` consecutive
+ * round trips, or max_rt round trips have run.  Asynchronous on stream. */
+cuopo_status cuopo_batch_run(cuopo_batch *batch, int max_rt, double tol, int patience, void *stream);
+/* Per-instance final signal power, round trips run and flag (1 converged,
+ * 0 round-trip limit, 5 non-finite) into host arrays (any may be NULL).
+ * Waits for stream. */
+cuopo_status cuopo_batch_results(cuopo_batch *batch, double *ps, int *rts, int *flags, void *stream);
+
 /* Blocks until the plan's work on stream has finished; returns the first
  * asynchronous error. */
 cuopo_status cuopo_sync(void *stream);

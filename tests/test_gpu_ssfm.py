@@ -5,7 +5,13 @@ Tolerances (relative L2 per field):
   F64 plan vs FP64 oracle ........ 1e-10 (pass and round trips)
   F32 plan vs FP64 oracle, pass .. 5e-6
   F32 plan vs FP64 oracle, rts ... 5e-5
-  F32 plan vs reference (cuFFT) .. 5e-6 pass, 5e-5 round trips
+  F32 plan vs reference (cuFFT) .. max(5e-5, 1.5 x the reference's own distance
+                                   from the FP64 oracle), and no farther from the
+                                   oracle than the reference itself
+The reference forms its spectral phases in float (CpxExp of a float argument,
+src/headers/operators.cuh:120-126); this library forms them in FP64, so where
+the phases are large (pump group-velocity term of the 3-wave NS case) the two
+FP32 results differ by the reference's own rounding error.
 """
 import numpy as np
 import pytest
@@ -228,12 +234,12 @@ def test_round_trips_vs_reference_cufft(neq, crystal, n_t, regime, kw):
     ob.ref_round_trips(crystal, q, w, T, pr[0], pr[1], pr[2], pump, n_rt, 0, n_rt)
     got, _, _, _ = run_rts(q, cu.F32, Ap, As, Ai, pump, n_rt, 0, n_rt, 0, 0)
     orc, _, _ = run_rts_oracle(q, Ap, As, Ai, pump, n_rt, 0, n_rt, 0, 0)
-    for g, r, o in zip(got, pr, orc):
+    errs = []
+    for name, g, r, o in zip(("pump", "signal", "idler"), got, pr, orc):
         if r is None:
             continue
-        e_ref = rel_l2(g, r)
-        e_ref_vs_oracle = rel_l2(r, o)
-        e_ours_vs_oracle = rel_l2(g, o)
-        assert e_ref < 5e-5, (e_ref, e_ref_vs_oracle, e_ours_vs_oracle)
-        # ours is at least as close to the FP64 oracle as the reference's own FP32 build
-        assert e_ours_vs_oracle < 2.0 * e_ref_vs_oracle + 1e-7
+        errs.append((name, rel_l2(g, r), rel_l2(r, o), rel_l2(g, o)))
+    for name, e_ref, e_ref_vs_oracle, e_ours_vs_oracle in errs:
+        assert e_ref < max(5e-5, 1.5 * e_ref_vs_oracle), errs
+        # ours is no farther from the FP64 oracle than the reference's own FP32 build
+        assert e_ours_vs_oracle < 1.2 * e_ref_vs_oracle + 2e-6, errs
