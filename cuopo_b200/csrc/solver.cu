@@ -25,10 +25,11 @@ struct cuopo_plan {
     int threads;      /* CTA size */
     int cluster;      /* CTAs per instance */
     size_t smem;      /* dynamic shared memory per CTA */
-    void *d_disp;     /* [F][N] */
+    void *d_disp;     /* [F][CL][M], entry [f][k2][k1] = D_f(k2 + CL k1) */
     void *d_rk;       /* [(n_z+1)][NCO] */
     void *d_eom;      /* [N] or NULL */
-    float *d_w;       /* [N] */
+    float *d_w;       /* [CL][M], same permutation */
+    void *d_twN;      /* [N] W_N^q (cluster plans) or NULL */
     int *d_status;
     double h6;
 };
@@ -55,79 +56,117 @@ extern "C" const char *cuopo_version(void) { return "cuopo_b200 0.1.0 (sm_100a)"
 
 /* -------------------------------------------------------- kernel registry */
 
-typedef cudaError_t (*launch_fn)(const LaunchArgs &, int grid, cudaStream_t);
+typedef cudaError_t (*launch_fn)(const LaunchArgs &, int clusters, cudaStream_t);
 typedef int (*occ_fn)(void);
 
-template <typename R, int F, int M, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
 static cudaError_t prepare_kernel()
 {
-    using K = Ssfm<R, F, M, INPLACE>;
-    static cudaError_t st = cudaFuncSetAttribute(ssfm_kernel<R, F, M, INPLACE, MINB>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)K::smem_bytes());
+    using K = Ssfm<R, F, M, CL, INPLACE>;
+    static cudaError_t st = [] {
+        cudaError_t e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, INPLACE, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem_bytes());
+        if (e == cudaSuccess && CL > 8)
+            e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, INPLACE, MINB>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        return e;
+    }();
     return st;
 }
 
-template <typename R, int F, int M, bool INPLACE, int MINB>
-static cudaError_t launch_impl(const LaunchArgs &a, int grid, cudaStream_t st)
+template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+static cudaLaunchConfig_t make_config(int clusters, cudaStream_t st, cudaLaunchAttribute *attr)
 {
-    using K = Ssfm<R, F, M, INPLACE>;
-    cudaError_t e = prepare_kernel<R, F, M, INPLACE, MINB>();
+    using K = Ssfm<R, F, M, CL, INPLACE>;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)(clusters * CL));
+    cfg.blockDim = dim3(K::T);
+    cfg.dynamicSmemBytes = K::smem_bytes();
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+static cudaError_t launch_impl(const LaunchArgs &a, int clusters, cudaStream_t st)
+{
+    cudaError_t e = prepare_kernel<R, F, M, CL, INPLACE, MINB>();
     if (e != cudaSuccess) return e;
-    ssfm_kernel<R, F, M, INPLACE, MINB><<<grid, K::T, K::smem_bytes(), st>>>(a);
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, INPLACE, MINB>(clusters, st, attr);
+    e = cudaLaunchKernelEx(&cfg, ssfm_kernel<R, F, M, CL, INPLACE, MINB>, a);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
-/* Resident CTAs per SM of this kernel (0 on error). */
-template <typename R, int F, int M, bool INPLACE, int MINB>
+/* Clusters (of CL CTAs) of this kernel that can be resident at once (0 on error). */
+template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
 static int occupancy_impl()
 {
-    using K = Ssfm<R, F, M, INPLACE>;
-    if (prepare_kernel<R, F, M, INPLACE, MINB>() != cudaSuccess) return 0;
+    if (prepare_kernel<R, F, M, CL, INPLACE, MINB>() != cudaSuccess) return 0;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, INPLACE, MINB>(1, 0, attr);
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ssfm_kernel<R, F, M, INPLACE, MINB>, K::T,
-                                                      K::smem_bytes()) != cudaSuccess)
-        return 0;
+    if (cudaOccupancyMaxActiveClusters(&n, ssfm_kernel<R, F, M, CL, INPLACE, MINB>, &cfg) != cudaSuccess) return 0;
     return n;
 }
 
 struct KernelEntry {
-    int precision, F, M;
+    int precision, F, M, CL;
     bool inplace;
     size_t smem;
     launch_fn fn;
     occ_fn occ;
 };
 
-#define CUOPO_K(R, PREC, F, M, IP, MINB)                                             \
-    {PREC, F, M, IP, Ssfm<R, F, M, IP>::smem_bytes(), &launch_impl<R, F, M, IP, MINB>, \
-     &occupancy_impl<R, F, M, IP, MINB>}
+#define CUOPO_K(R, PREC, F, M, CL, IP, MINB)                                                  \
+    {PREC, F, M, CL, IP, Ssfm<R, F, M, CL, IP>::smem_bytes(), &launch_impl<R, F, M, CL, IP, MINB>, \
+     &occupancy_impl<R, F, M, CL, IP, MINB>}
 
+/* Built configurations; the first entry with M * CL == n_t is used. */
 static const KernelEntry k_kernels[] = {
-    CUOPO_K(float, CUOPO_F32, 2, 512, false, 1),
-    CUOPO_K(float, CUOPO_F32, 2, 1024, false, 1),
-    CUOPO_K(float, CUOPO_F32, 2, 2048, false, 1),
-    CUOPO_K(float, CUOPO_F32, 2, 4096, false, 2),
-    CUOPO_K(float, CUOPO_F32, 2, 8192, false, 1),
-    CUOPO_K(float, CUOPO_F32, 3, 512, false, 1),
-    CUOPO_K(float, CUOPO_F32, 3, 1024, false, 1),
-    CUOPO_K(float, CUOPO_F32, 3, 2048, false, 1),
-    CUOPO_K(float, CUOPO_F32, 3, 4096, false, 1),
-    CUOPO_K(float, CUOPO_F32, 3, 8192, true, 1),
-    CUOPO_K(double, CUOPO_F64, 2, 512, false, 1),
-    CUOPO_K(double, CUOPO_F64, 2, 1024, false, 1),
-    CUOPO_K(double, CUOPO_F64, 2, 2048, false, 1),
-    CUOPO_K(double, CUOPO_F64, 2, 4096, false, 1),
-    CUOPO_K(double, CUOPO_F64, 3, 512, false, 1),
-    CUOPO_K(double, CUOPO_F64, 3, 1024, false, 1),
-    CUOPO_K(double, CUOPO_F64, 3, 2048, false, 1),
-    CUOPO_K(double, CUOPO_F64, 3, 4096, true, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 512, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 1024, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 2048, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 4096, 1, false, 2),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 2, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 4, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 8, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 512, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 1024, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 2048, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 4096, 1, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 8192, 1, true, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 4096, 4, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 4096, 8, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 4096, 16, false, 1),
+    CUOPO_K(float, CUOPO_F32, 3, 8192, 16, true, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 512, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 1024, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 2048, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, 2, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, 4, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, 8, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 512, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 1024, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 2048, 1, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 4096, 1, true, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 2048, 8, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 4096, 16, true, 1),
 };
 
 static const KernelEntry *find_kernel(int precision, int F, int N)
 {
     for (const KernelEntry &k : k_kernels)
-        if (k.precision == precision && k.F == F && k.M == N) return &k;
+        if (k.precision == precision && k.F == F && k.M * k.CL == N) return &k;
     return nullptr;
 }
 
@@ -153,9 +192,10 @@ static void stage_times(const cuopo_params &p, int s_count, std::vector<double> 
 }
 
 template <typename R>
-static std::vector<unsigned char> build_tables(const cuopo_params &p, const float *w, const float *T,
+static std::vector<unsigned char> build_tables(const cuopo_params &p, const float *w, const float *T, int CL,
                                                std::vector<unsigned char> &rk_out,
-                                               std::vector<unsigned char> &eom_out, double &h6)
+                                               std::vector<unsigned char> &eom_out,
+                                               std::vector<unsigned char> &twn_out, double &h6)
 {
     using C = cpx<R>;
     const int N = p.n_t;
@@ -178,12 +218,25 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
     std::vector<unsigned char> disp(sizeof(C) * (size_t)F * N);
     C *D = reinterpret_cast<C *>(disp.data());
     const double z = p.dz;
+    const int M = N / CL;
     for (int f = 0; f < F; f++) {
         const double att = std::exp(-0.5 * al[f] * z) / (double)N;
         for (int k = 0; k < N; k++) {
             const double wk = (double)w[k];
             const double ph = z * wk * (gvm[f] + 0.5 * wk * b2[f] + wk * wk * b3[f] / 6.0);
-            D[(size_t)f * N + k] = mk<C>((R)(std::cos(ph) * att), (R)(std::sin(ph) * att));
+            /* frequency k = k2 + CL k1 is entry k1 of CTA k2's row */
+            const int k2 = k % CL, k1 = k / CL;
+            D[(size_t)f * N + (size_t)k2 * M + k1] = mk<C>((R)(std::cos(ph) * att), (R)(std::sin(ph) * att));
+        }
+    }
+    /* cross-stage twiddles W_N^q = exp(2 pi i q / N) */
+    twn_out.clear();
+    if (CL > 1) {
+        twn_out.resize(sizeof(C) * (size_t)N);
+        C *W = reinterpret_cast<C *>(twn_out.data());
+        for (int q = 0; q < N; q++) {
+            const double a = 2.0 * M_PI * (double)q / (double)N;
+            W[q] = mk<C>((R)std::cos(a), (R)std::sin(a));
         }
     }
     /* RK4 stage coefficients per slice (one extra zero row at the end). */
@@ -259,10 +312,14 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
         if (st != CUOPO_OK) return st;
     }
 
-    std::vector<unsigned char> disp, rk, eom;
+    std::vector<unsigned char> disp, rk, eom, twn;
     double h6 = 0;
-    if (precision == CUOPO_F32) disp = build_tables<float>(*p, w.data(), T.data(), rk, eom, h6);
-    else disp = build_tables<double>(*p, w.data(), T.data(), rk, eom, h6);
+    const int CL = k->CL;
+    if (precision == CUOPO_F32) disp = build_tables<float>(*p, w.data(), T.data(), CL, rk, eom, twn, h6);
+    else disp = build_tables<double>(*p, w.data(), T.data(), CL, rk, eom, twn, h6);
+    /* frequency grid in the same per-CTA order as the dispersion table */
+    std::vector<float> wp((size_t)p->n_t);
+    for (int q = 0; q < p->n_t; q++) wp[(size_t)(q % CL) * (p->n_t / CL) + q / CL] = w[q];
 
     cuopo_plan *pl = new (std::nothrow) cuopo_plan();
     if (!pl) return cuopo_fail(CUOPO_ENOMEM, "plan_create: out of host memory");
@@ -271,7 +328,7 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
     pl->F = p->n_eqs;
     pl->N = p->n_t;
     pl->threads = k->M / 16;
-    pl->cluster = 1;
+    pl->cluster = k->CL;
     pl->smem = k->smem;
     pl->h6 = h6;
     cudaError_t e;
@@ -279,16 +336,18 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
         (e = cudaMalloc(&pl->d_rk, rk.size())) != cudaSuccess ||
         (e = cudaMalloc(&pl->d_w, sizeof(float) * p->n_t)) != cudaSuccess ||
         (e = cudaMalloc(&pl->d_status, sizeof(int))) != cudaSuccess ||
-        (!eom.empty() && (e = cudaMalloc(&pl->d_eom, eom.size())) != cudaSuccess)) {
+        (!eom.empty() && (e = cudaMalloc(&pl->d_eom, eom.size())) != cudaSuccess) ||
+        (!twn.empty() && (e = cudaMalloc(&pl->d_twN, twn.size())) != cudaSuccess)) {
         cuopo_plan_destroy(pl);
         return e == cudaErrorMemoryAllocation ? cuopo_fail(CUOPO_ENOMEM, "plan_create: device allocation failed")
                                               : cuda_fail(e, "plan_create: cudaMalloc");
     }
     if ((e = cudaMemcpy(pl->d_disp, disp.data(), disp.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(pl->d_rk, rk.data(), rk.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(pl->d_w, w.data(), sizeof(float) * p->n_t, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(pl->d_w, wp.data(), sizeof(float) * p->n_t, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(pl->d_status, 0, sizeof(int))) != cudaSuccess ||
-        (!eom.empty() && (e = cudaMemcpy(pl->d_eom, eom.data(), eom.size(), cudaMemcpyHostToDevice)) != cudaSuccess)) {
+        (!eom.empty() && (e = cudaMemcpy(pl->d_eom, eom.data(), eom.size(), cudaMemcpyHostToDevice)) != cudaSuccess) ||
+        (!twn.empty() && (e = cudaMemcpy(pl->d_twN, twn.data(), twn.size(), cudaMemcpyHostToDevice)) != cudaSuccess)) {
         cuopo_plan_destroy(pl);
         return cuda_fail(e, "plan_create: upload");
     }
@@ -303,6 +362,7 @@ extern "C" cuopo_status cuopo_plan_destroy(cuopo_plan *pl)
     cudaFree(pl->d_rk);
     cudaFree(pl->d_eom);
     cudaFree(pl->d_w);
+    cudaFree(pl->d_twN);
     cudaFree(pl->d_status);
     delete pl;
     return CUOPO_OK;
@@ -325,6 +385,7 @@ static LaunchArgs base_args(const cuopo_plan *pl)
     a.tab.rk = pl->d_rk;
     a.tab.eom = pl->d_eom;
     a.tab.w = pl->d_w;
+    a.tab.twN = pl->d_twN;
     a.tab.h6 = pl->h6;
     a.tab.inv_n = 1.0 / (double)pl->N;
     a.n_z = pl->p.n_z;
@@ -542,16 +603,14 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
         for (int i = 0; i < count; i++)
             if (inst[i].n_t == n_t) g.members.push_back(i);
         const KernelEntry *k = find_kernel(precision, 2, n_t);
-        int occ = k->occ();
+        /* persistent grid: as many clusters as can be resident at once */
+        const int occ = k->occ();
         if (occ < 1) {
             b->groups.push_back(g);
             cuopo_batch_destroy(b);
-            return cuopo_fail(CUOPO_ECUDA, "batch_create: kernel does not fit on an SM");
+            return cuopo_fail(CUOPO_ECUDA, "batch_create: kernel does not fit on the device");
         }
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        g.grid = std::min((int)g.members.size(), occ * sms);
+        g.grid = std::min((int)g.members.size(), occ);
         if ((e = cudaMalloc(&g.d_inst, sizeof(Instance) * g.members.size())) != cudaSuccess ||
             (e = cudaMalloc(&g.d_queue, sizeof(int))) != cudaSuccess ||
             (e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||

@@ -1,9 +1,10 @@
 /*
- * ssfm.cuh -- the fused SSFM round-trip kernel (one CTA per OPO instance).
+ * ssfm.cuh -- the fused SSFM round-trip kernel.
  *
  * One launch runs whole crystal passes and cavity round trips of the
- * reference loop (src/cuOPO.cu:474-610) with every field resident in
- * shared memory:
+ * reference loop (src/cuOPO.cu:474-610) with every field resident in shared
+ * memory, for one instance per CTA (CL = 1) or per thread-block cluster of
+ * CL CTAs (grids up to CL x 8192 points):
  *
  *   per round trip:  pump injection (cuOPO.cu:478-486, functions.cuh:191-213)
  *     per slice s:   RK4 half step at z_s (cwes2.cuh:147-166)
@@ -15,10 +16,18 @@
  *     (functions.cuh:139-152), SaveRoundTrip (functions.cuh:217-238), and
  *     the signal power for the convergence rule.
  *
- * The second half step of slice s and the first of slice s+1 are applied
- * back to back in one element-wise phase.  Element-wise phases touch only
- * the points t + e*T of each field that thread t holds before and after
- * every transform, so they need no barrier.
+ * Cluster decomposition (N = CL * M): CTA c holds time block n = n1 + M c.
+ * The T->W transform is a radix-CL "cross" stage over the CTAs,
+ *   y_k2[n1] = W_N^{n1 k2} sum_n2 x[n1 + M n2] W_CL^{n2 k2}   (stored on CTA k2),
+ * followed by a local M-point transform on CTA k2 giving X[k2 + CL k1]; the
+ * W->T transform runs the same two steps backwards.  Between the local W->T
+ * transform of slice s and the local T->W transform of slice s+1 the
+ * inverse cross stage, both RK4 half steps and the forward cross stage are
+ * one element-wise pass over distributed shared memory, so each slice costs
+ * one exchange between the CTAs and two cluster barriers.  The fields live
+ * in the y domain between slices; the time domain exists only inside that
+ * pass (and at round-trip ends).  With CL = 1 the cross stages are
+ * identities and no barrier is needed around the element-wise passes.
  *
  * Quirks kept: RK4 stages use aux = A + s k without the step (Q1); both
  * half steps of a slice use the same z (Q2); in the 3-equation model all
@@ -26,16 +35,21 @@
  * A += c(z) * P(A) with one complex coefficient per field and slice.
  */
 #pragma once
+#include <cooperative_groups.h>
+
 #include "fft.cuh"
 
 namespace cuopo {
 
-/* Per-plan device tables (type-erased; element type is cpx<R>). */
+/* Per-plan device tables (type-erased; element type is cpx<R>).  Tables
+ * indexed by frequency are stored per CTA: entry [k2][k1] is frequency
+ * index k2 + CL k1. */
 struct Tables {
-    const void *disp;   /* [F][N]: slice dispersion x attenuation / N */
-    const void *rk;     /* [n_z][6] (2 eqs) or [n_z][3] (3 eqs) RK4 coefficients */
+    const void *disp;   /* [F][CL][M]: slice dispersion x attenuation / N */
+    const void *rk;     /* [n_z + 1][6] (2 eqs) or [n_z + 1][3] (3 eqs) RK4 coefficients */
     const void *eom;    /* [N]: exp(i m sin(2 pi fpm T)) or NULL */
-    const float *w;     /* [N]: angular frequency grid (reference float values) */
+    const float *w;     /* [CL][M]: angular frequency grid (reference float values) */
+    const void *twN;    /* [N]: W_N^q (cross-stage twiddles; CL > 1) */
     double h6;          /* (dz/2)/6 */
     double inv_n;       /* 1/N */
 };
@@ -120,26 +134,156 @@ __device__ __forceinline__ void rk4_half3(C &Ap, C &As, C &Ai, const C *__restri
     Ai = cadd(Ai, cmul(co[2], Pi));
 }
 
-template <typename R, int F, int M, bool INPLACE>
+
+namespace cg = cooperative_groups;
+
+template <typename R, int F, int M, int CL, bool INPLACE>
 struct Ssfm {
     using C = cpx<R>;
     using SP = StagePlan<M>;
     static constexpr int T = SP::T;
     static constexpr int P = SP::P;
+    static constexpr int N = M * CL;
+    static constexpr int J = 16 / CL;  /* n1 values per thread in a cross stage */
     static constexpr int NCO = (F == 2) ? 6 : 3;
+    static constexpr unsigned ALL = (1u << F) - 1u;
+    static_assert(CL == 1 || CL == 2 || CL == 4 || CL == 8 || CL == 16, "cluster size must be 1..16, power of 2");
 
     /* Shared memory: home[F][M] (+ scratch[M]) complex values, then the
      * twiddle table of the middle FFT stages. */
     static constexpr size_t field_elems() { return (size_t)M * (F + (INPLACE ? 0 : 1)); }
     static constexpr size_t smem_bytes() { return sizeof(C) * (field_elems() + TwTable<M>::size()); }
 
-    /* T->W, multiply by the table row (or the on-the-fly GDD factor),
-     * W->T, on the field at home. */
-    template <int MODE>  /* 0: table row mul, 1: GDD with TOD flag */
+    /* Element-wise work of one cross stage (uniform over the cluster). */
+    struct Ops {
+        int inject;         /* pump injection */
+        long poff;          /* NS pump window offset of this round trip */
+        const C *rk0, *rk1; /* RK4 half steps to apply (NULL: none) */
+        int eom;            /* intracavity phase modulator */
+        int addphase;       /* AddPhase on the resonant fields */
+        C ph_s, ph_i;
+        int save;           /* SaveRoundTrip into slot */
+        size_t slot;
+        int power;          /* accumulate |As|^2 */
+    };
+
+    static __device__ __forceinline__ void xsync()
+    {
+        if constexpr (CL > 1) cg::this_cluster().sync();
+    }
+
+    static __device__ __forceinline__ void bar()
+    {
+        if constexpr (CL > 1) cg::this_cluster().sync();
+        else __syncthreads();
+    }
+
+    template <typename X>
+    static __device__ __forceinline__ X *peer(X *p, int rank)
+    {
+        if constexpr (CL == 1) return p;
+        else return cg::this_cluster().map_shared_rank(p, rank);
+    }
+
+    static __device__ __forceinline__ void pointwise(C (&A)[3], int n, const Ops &op, const Instance &I,
+                                                     const Tables &tab, R h6, int eom_idler, double &acc)
+    {
+        if (op.inject) A[0] = I.pump ? ldc<C>(I.pump, op.poff + n) : mk<C>((R)I.ap0, (R)0);
+        if (op.rk0) {
+            if constexpr (F == 2) rk4_half2(A[0], A[1], op.rk0, h6);
+            else rk4_half3(A[0], A[1], A[2], op.rk0);
+        }
+        if (op.rk1) {
+            if constexpr (F == 2) rk4_half2(A[0], A[1], op.rk1, h6);
+            else rk4_half3(A[0], A[1], A[2], op.rk1);
+        }
+        if (op.eom) {
+            const C ef = ldc<C>(tab.eom, n);
+            A[1] = cmul(A[1], ef);
+            if (F == 3 && eom_idler) A[F - 1] = cmul(A[F - 1], ef);
+        }
+        if (op.addphase) {
+            A[1] = cmul(A[1], op.ph_s);
+            if constexpr (F == 3) A[2] = cmul(A[2], op.ph_i);
+        }
+        if (op.save) {
+            C *sv[3] = {reinterpret_cast<C *>(I.sv_p), reinterpret_cast<C *>(I.sv_s),
+                        reinterpret_cast<C *>(I.sv_i)};
+#pragma unroll
+            for (int f = 0; f < F; f++)
+                if (sv[f]) sv[f][op.slot + n] = A[f];
+        }
+        if (op.power) acc += cabs2d(A[1]);
+    }
+
+    /* One element-wise pass over the cluster.  Fields with their bit set in
+     * in_y are read in the y domain (inverse cross stage applied), the
+     * others as time values; out_y likewise for the write-back.  Thread t
+     * of CTA `rank` owns positions n1 = rank M/CL + t + j T, j < J, in every
+     * CTA's home; it reads and writes only those. */
+    static __device__ __forceinline__ void cross(C *home, unsigned in_y, unsigned out_y, const Ops &op,
+                                                 const Instance &I, const Tables &tab, R h6, int eom_idler,
+                                                 double &acc, int t, int rank)
+    {
+        const C *__restrict__ twN = reinterpret_cast<const C *>(tab.twN);
+#pragma unroll 1
+        for (int j = 0; j < J; j++) {
+            const int n1 = rank * (M / CL) + t + j * T;
+            const int sm = swz<C>(n1);
+            C v[3][CL];
+#pragma unroll
+            for (int c = 0; c < CL; c++) {
+                const C *src = peer(home, c);
+#pragma unroll
+                for (int f = 0; f < F; f++) v[f][c] = src[f * M + sm];
+            }
+            C w[CL];
+            if constexpr (CL > 1) {
+#pragma unroll
+                for (int c = 1; c < CL; c++) w[c] = __ldg(twN + (long)n1 * c);
+#pragma unroll
+                for (int f = 0; f < F; f++) {
+                    if ((in_y >> f) & 1u) {
+#pragma unroll
+                        for (int c = 1; c < CL; c++) v[f][c] = cmulc(v[f][c], w[c]);
+                        dft<-1, CL>(v[f]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CL; c++) {
+                C A[3];
+#pragma unroll
+                for (int f = 0; f < F; f++) A[f] = v[f][c];
+                pointwise(A, n1 + M * c, op, I, tab, h6, eom_idler, acc);
+#pragma unroll
+                for (int f = 0; f < F; f++) v[f][c] = A[f];
+            }
+            if constexpr (CL > 1) {
+#pragma unroll
+                for (int f = 0; f < F; f++) {
+                    if ((out_y >> f) & 1u) {
+                        dft<+1, CL>(v[f]);
+#pragma unroll
+                        for (int c = 1; c < CL; c++) v[f][c] = cmul(v[f][c], w[c]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CL; c++) {
+                C *dst = peer(home, c);
+#pragma unroll
+                for (int f = 0; f < F; f++) dst[f * M + sm] = v[f][c];
+            }
+        }
+    }
+
+    /* Local T->W, multiply by a table row (or the GDD factor), local W->T. */
+    template <int MODE> /* 0: table row, 1: GDD/TOD factor formed in FP64 */
     static __device__ __forceinline__ void spectral(C *home, C *scratch, const C *__restrict__ row,
-                                                    const float *__restrict__ w, double gdd,
-                                                    double tod, int use_tod, double inv_n,
-                                                    const StageTwiddles<M, C> &tw, int t)
+                                                    const float *__restrict__ w, double gdd, double tod,
+                                                    int use_tod, double inv_n, const StageTwiddles<M, C> &tw,
+                                                    int t)
     {
         C reg[16];
         load_own<M>(home, reg, t);
@@ -152,13 +296,12 @@ struct Ssfm {
         } else {
 #pragma unroll 4
             for (int e = 0; e < 16; e++) {
-                /* functions.cuh:156-186 with CUFFTscale folded in, formed in FP64 */
+                /* functions.cuh:156-186 with CUFFTscale folded in */
                 const double wk = (double)__ldg(w + t + e * T);
-                const double ph = use_tod ? 0.5 * wk * (wk * gdd + wk * wk * tod / 3.0)
-                                          : 0.5 * wk * wk * gdd;
-                double s, c;
-                sincos(ph, &s, &c);
-                reg[e] = cmul(reg[e], mk<C>((R)(c * inv_n), (R)(s * inv_n)));
+                const double ph = use_tod ? 0.5 * wk * (wk * gdd + wk * wk * tod / 3.0) : 0.5 * wk * wk * gdd;
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                reg[e] = cmul(reg[e], mk<C>((R)(cs * inv_n), (R)(sn * inv_n)));
             }
         }
         local_transform<-1, M, P - 1, INPLACE>(reg, bufA, bufB, tw, t);
@@ -184,147 +327,128 @@ struct Ssfm {
         C *home = reinterpret_cast<C *>(smem_raw);
         C *scratch = INPLACE ? home : home + (size_t)F * M;
         __shared__ double red[32];
+        __shared__ double red_cl;
         __shared__ int next_inst;
         const int t = threadIdx.x;
+        int rank = 0;
+        if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
 
         C *twtab = home + field_elems();
         fill_twiddle_table<M>(twtab, t);
         StageTwiddles<M, C> tw;
         tw.init(t, twtab);
         __syncthreads();
-        const R h6 = (R)a.tab.h6;
-        const C *__restrict__ rk = reinterpret_cast<const C *>(a.tab.rk);
-        const C *__restrict__ disp = reinterpret_cast<const C *>(a.tab.disp);
-        const C *__restrict__ eomt = reinterpret_cast<const C *>(a.tab.eom);
+        const Tables &tab = a.tab;
+        const R h6 = (R)tab.h6;
+        const C *__restrict__ rk = reinterpret_cast<const C *>(tab.rk);
+        const C *__restrict__ disp = reinterpret_cast<const C *>(tab.disp);
+        const float *__restrict__ wtab = tab.w + (size_t)rank * M;
 
-        int idx = a.inst ? -1 : (int)blockIdx.x;
+        bool first = true;
         for (;;) {
+            int idx;
             if (a.inst) {
-                if (a.queue) {
-                    if (t == 0) next_inst = atomicAdd(a.queue, 1);
-                    __syncthreads();
-                    idx = next_inst;
-                    __syncthreads();
-                } else {
-                    idx = (idx < 0) ? (int)blockIdx.x : idx + (int)gridDim.x;
-                }
+                if (rank == 0 && t == 0) next_inst = atomicAdd(a.queue, 1);
+                bar();
+                idx = *peer(&next_inst, 0);
+                bar();
                 if (idx >= a.n_inst) break;
-            } else if (idx != 0) {
-                break;
+            } else {
+                if (!first) break;
+                idx = 0;
             }
+            first = false;
             const Instance &I = a.inst ? a.inst[idx] : a.single;
 
-            C *gf[3] = {reinterpret_cast<C *>(I.Ap), reinterpret_cast<C *>(I.As),
-                        reinterpret_cast<C *>(I.Ai)};
+            C *gf[3] = {reinterpret_cast<C *>(I.Ap), reinterpret_cast<C *>(I.As), reinterpret_cast<C *>(I.Ai)};
 #pragma unroll
             for (int f = 0; f < F; f++)
 #pragma unroll
-                for (int e = 0; e < 16; e++) home[f * M + swz<C>(t + e * T)] = gf[f][t + e * T];
+                for (int e = 0; e < 16; e++)
+                    home[f * M + swz<C>(t + e * T)] = gf[f][(size_t)rank * M + t + e * T];
+            xsync();
 
-            double prev_ps = -1.0, ps = 0.0;
+            double prev_ps = -1.0, ps = 0.0, acc = 0.0;
             int rts = 0, calm = 0, flag = 0;
             bool stop = false;
+            const C *last_row = rk + (size_t)(a.n_z - 1) * NCO;
             for (int rt = I.rt_begin; rt < I.rt_begin + I.rt_count && !stop; rt++) {
-                /* pump injection + first half step of slice 0 */
                 {
-                    long poff = 0;
+                    Ops op{};
+                    op.inject = !a.pass_only;
                     if (a.regime == 1) {
                         /* ReadPump offsets, functions.cuh:196-210 (Q6) */
                         const int nrt = I.n_rt_total;
-                        poff = (rt == 0) ? 0 : ((rt > 0 && rt < nrt - 1) ? (long)rt * M
-                                                                         : (long)M * nrt - 1 - M);
+                        op.poff = (rt == 0) ? 0 : ((rt > 0 && rt < nrt - 1) ? (long)rt * N : (long)N * nrt - 1 - N);
                     }
-#pragma unroll 2
-                    for (int e = 0; e < 16; e++) {
-                        const int m = t + e * T;
-                        const int sm = swz<C>(m);
-                        C A[3];
-#pragma unroll
-                        for (int f = 0; f < F; f++) A[f] = home[f * M + sm];
-                        if (!a.pass_only) {
-                            if (I.pump) A[0] = ldc<C>(I.pump, poff + m);
-                            else A[0] = mk<C>((R)I.ap0, (R)0);
-                        }
-                        if constexpr (F == 2) rk4_half2(A[0], A[1], rk, h6);
-                        else rk4_half3(A[0], A[1], A[2], rk);
-#pragma unroll
-                        for (int f = 0; f < F; f++) home[f * M + sm] = A[f];
-                    }
+                    op.rk0 = rk;
+                    cross(home, 0u, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    xsync();
                 }
                 for (int s = 0; s < a.n_z; s++) {
 #pragma unroll 1
                     for (int f = 0; f < F; f++)
-                        spectral<0>(home + f * M, scratch, disp + (size_t)f * M, nullptr, 0.0, 0.0,
+                        spectral<0>(home + f * M, scratch, disp + ((size_t)f * CL + rank) * M, nullptr, 0.0, 0.0,
                                     0, 0.0, tw, t);
-                    const C *co0 = rk + (size_t)s * NCO;
-                    const C *co1 = rk + (size_t)(s + 1) * NCO;
-                    const bool next = (s + 1 < a.n_z);
-                    const bool eom = (!next && !a.pass_only && a.use_eom);
-#pragma unroll 2
-                    for (int e = 0; e < 16; e++) {
-                        const int m = t + e * T;
-                        const int sm = swz<C>(m);
-                        C A[3];
-#pragma unroll
-                        for (int f = 0; f < F; f++) A[f] = home[f * M + sm];
-                        if constexpr (F == 2) {
-                            rk4_half2(A[0], A[1], co0, h6);
-                            if (next) rk4_half2(A[0], A[1], co1, h6);
-                        } else {
-                            rk4_half3(A[0], A[1], A[2], co0);
-                            if (next) rk4_half3(A[0], A[1], A[2], co1);
-                        }
-                        if (eom) {
-                            const C ef = __ldg(eomt + m);
-                            A[1] = cmul(A[1], ef);
-                            if (F == 3 && a.eom_idler) A[F - 1] = cmul(A[F - 1], ef);
-                        }
-#pragma unroll
-                        for (int f = 0; f < F; f++) home[f * M + sm] = A[f];
+                    xsync();
+                    if (s + 1 < a.n_z) {
+                        Ops op{};
+                        op.rk0 = rk + (size_t)s * NCO;
+                        op.rk1 = rk + (size_t)(s + 1) * NCO;
+                        cross(home, ALL, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                        xsync();
                     }
                 }
                 rts++;
-                if (a.pass_only) break;
-
-                /* GDD / TOD compensation of the resonant fields (cuOPO.cu:521-553) */
-                if (I.gdd != 0.0) {
-                    spectral<1>(home + 1 * M, scratch, nullptr, a.tab.w, I.gdd, I.tod_s, I.use_tod_s,
-                                a.tab.inv_n, tw, t);
-                    if constexpr (F == 3)
-                        spectral<1>(home + 2 * M, scratch, nullptr, a.tab.w, I.gdd, I.tod_i,
-                                    I.use_tod_i, a.tab.inv_n, tw, t);
+                if (a.pass_only) {
+                    Ops op{};
+                    op.rk0 = last_row;
+                    cross(home, ALL, 0u, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    xsync();
+                    break;
                 }
-
-                /* AddPhase, SaveRoundTrip, signal power */
-                const C ph_s = mk<C>((R)I.phase_s[0], (R)I.phase_s[1]);
-                const C ph_i = mk<C>((R)I.phase_i[0], (R)I.phase_i[1]);
                 const bool save = (rt >= I.save_first && rt < I.save_first + I.save_count);
-                const size_t slot = save ? (size_t)(rt - I.save_first) * M : 0;
-                C *sv[3] = {reinterpret_cast<C *>(I.sv_p), reinterpret_cast<C *>(I.sv_s),
-                            reinterpret_cast<C *>(I.sv_i)};
-                double acc = 0.0;
-#pragma unroll 2
-                for (int e = 0; e < 16; e++) {
-                    const int m = t + e * T;
-                    const int sm = swz<C>(m);
-                    C A[3];
-#pragma unroll
-                    for (int f = 0; f < F; f++) A[f] = home[f * M + sm];
-                    A[1] = cmul(A[1], ph_s);
-                    if constexpr (F == 3) A[2] = cmul(A[2], ph_i);
-                    home[1 * M + sm] = A[1];
-                    if constexpr (F == 3) home[2 * M + sm] = A[2];
-                    if (save) {
-#pragma unroll
-                        for (int f = 0; f < F; f++)
-                            if (sv[f]) sv[f][slot + m] = A[f];
-                    }
-                    acc += cabs2d(A[1]);
+                Ops end{};
+                end.addphase = 1;
+                end.ph_s = mk<C>((R)I.phase_s[0], (R)I.phase_s[1]);
+                end.ph_i = mk<C>((R)I.phase_i[0], (R)I.phase_i[1]);
+                end.save = save;
+                end.slot = save ? (size_t)(rt - I.save_first) * N : 0;
+                end.power = 1;
+                acc = 0.0;
+                if (I.gdd != 0.0) {
+                    /* GDD / TOD compensation of the resonant fields (cuOPO.cu:521-553):
+                     * signal and idler go to the frequency domain, the pump stays in time */
+                    Ops op{};
+                    op.rk0 = last_row;
+                    op.eom = a.use_eom;
+                    const unsigned res = ALL & ~1u;
+                    cross(home, ALL, res, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    xsync();
+                    spectral<1>(home + 1 * M, scratch, nullptr, wtab, I.gdd, I.tod_s, I.use_tod_s, tab.inv_n, tw, t);
+                    if constexpr (F == 3)
+                        spectral<1>(home + 2 * M, scratch, nullptr, wtab, I.gdd, I.tod_i, I.use_tod_i, tab.inv_n, tw,
+                                    t);
+                    xsync();
+                    cross(home, res, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
+                } else {
+                    end.rk0 = last_row;
+                    end.eom = a.use_eom;
+                    cross(home, ALL, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 }
-                ps = block_sum(acc, red, t) * a.tab.inv_n;
-                if (t == 0 && I.ps_hist) I.ps_hist[rt - I.rt_begin] = ps;
+                /* signal power over the cluster, summed in rank order by every CTA */
+                double part = block_sum(acc, red, t);
+                if constexpr (CL > 1) {
+                    if (t == 0) red_cl = part;
+                    cg::this_cluster().sync();
+                    part = 0.0;
+#pragma unroll
+                    for (int c = 0; c < CL; c++) part += *peer(&red_cl, c);
+                }
+                ps = part * tab.inv_n;
+                if (rank == 0 && t == 0 && I.ps_hist) I.ps_hist[rt - I.rt_begin] = ps;
                 if (!(ps == ps) || ps > 1.0e300) {
-                    if (t == 0 && a.status) atomicCAS(a.status, 0, (int)ST_NONFINITE);
+                    if (rank == 0 && t == 0 && a.status) atomicCAS(a.status, 0, (int)ST_NONFINITE);
                     flag = ST_NONFINITE;
                     stop = true;
                 }
@@ -343,22 +467,22 @@ struct Ssfm {
 #pragma unroll
             for (int f = 0; f < F; f++)
 #pragma unroll
-                for (int e = 0; e < 16; e++) gf[f][t + e * T] = home[f * M + swz<C>(t + e * T)];
-            if (t == 0) {
+                for (int e = 0; e < 16; e++)
+                    gf[f][(size_t)rank * M + t + e * T] = home[f * M + swz<C>(t + e * T)];
+            if (rank == 0 && t == 0) {
                 if (I.rt_done) *I.rt_done = rts;
                 if (I.ps_out) *I.ps_out = ps;
                 if (I.flag_out) *I.flag_out = flag;
             }
-            __syncthreads();
-            if (!a.inst) break;
+            bar();
         }
     }
 };
 
-template <typename R, int F, int M, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
 __global__ void __launch_bounds__(M / 16, MINB) ssfm_kernel(const LaunchArgs a)
 {
-    Ssfm<R, F, M, INPLACE>::run(a);
+    Ssfm<R, F, M, CL, INPLACE>::run(a);
 }
 
 }  // namespace cuopo

@@ -58,9 +58,11 @@ def run_pass_oracle(p, Ap, As, Ai):
     return A
 
 
-CASES_F64 = [(2, 512), (2, 1024), (2, 2048), (2, 4096), (3, 512), (3, 1024), (3, 2048), (3, 4096)]
+# single-CTA grids and cluster grids (2-16 CTAs with distributed shared memory)
+CASES_F64 = [(2, 512), (2, 1024), (2, 2048), (2, 4096), (3, 512), (3, 1024), (3, 2048), (3, 4096),
+             (2, 8192), (2, 16384), (2, 32768), (3, 16384), (3, 65536)]
 CASES_F32 = [(2, 512), (2, 1024), (2, 2048), (2, 4096), (2, 8192), (3, 512), (3, 1024), (3, 2048), (3, 4096),
-             (3, 8192)]
+             (3, 8192), (2, 16384), (2, 32768), (2, 65536), (3, 16384), (3, 32768), (3, 65536), (3, 131072)]
 
 
 def make_params(neq, n_t, **kw):
@@ -129,6 +131,9 @@ RT_CASES = [
     (3, 1024, cu.NS, dict(gdd_percent=40.0, delta=0.05)),
     (3, 2048, cu.NS, dict()),
     (3, 1024, cu.CW, dict(delta=0.1)),
+    (2, 16384, cu.CW, dict(delta=0.03, gdd_percent=30.0, use_eom=1)),
+    (2, 32768, cu.CW, dict(r_percent=95.0)),
+    (3, 65536, cu.NS, dict(gdd_percent=20.0)),
 ]
 
 
@@ -146,8 +151,7 @@ def rt_inputs(neq, n_t, regime, kw, seed):
 @pytest.mark.parametrize("prec", [cu.F64, cu.F32])
 @pytest.mark.parametrize("neq,n_t,regime,kw", RT_CASES)
 def test_round_trips_vs_oracle(prec, neq, n_t, regime, kw):
-    if prec == cu.F64 and n_t > 4096:
-        pytest.skip("no F64 kernel above 4096 points per CTA")
+
     p, n_rt, Ap, As, Ai, pump = rt_inputs(neq, n_t, regime, kw, 100 + n_t)
     c = (lambda a: None if a is None else a.astype(np.complex64).astype(np.complex128))
     if prec == cu.F32:
