@@ -108,7 +108,11 @@ SIGNATURES = {
     "cuopo_batch_set_signal": (_i, [_vp, _vp, _i, _vp]),
     "cuopo_batch_get_signal": (_i, [_vp, _vp, _i, _vp]),
     "cuopo_batch_run": (_i, [_vp, _i, _d, _i, _vp]),
+    "cuopo_batch_reset": (_i, [_vp, _vp]),
+    "cuopo_batch_step": (_i, [_vp, _i, _i, _d, _i, _vp]),
+    "cuopo_batch_pending": (_i, [_vp, C.POINTER(_i), _vp]),
     "cuopo_batch_results": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "cuopo_probe_fp32_peak": (_i, [C.POINTER(_d), _vp]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

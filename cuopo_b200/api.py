@@ -205,6 +205,13 @@ def fft_c2c(x, sign: int, out=None, stream=None):
     return out
 
 
+def probe_fp32_peak(stream=None) -> float:
+    """Measured FP32 FMA throughput of the current device [TFLOP/s]."""
+    v = C.c_double()
+    check(load().cuopo_probe_fp32_peak(C.byref(v), _stream(stream)))
+    return v.value
+
+
 def sync(stream=None) -> None:
     check(load().cuopo_sync(_stream(stream) if stream is not None else None))
 
@@ -263,7 +270,20 @@ class Batch:
             check(self._lib.cuopo_batch_get_signal(self._h, dst.data_ptr(), int(dst.is_cuda), _stream(stream)))
 
     def run(self, max_rt: int, tol: float, patience: int = 1, stream=None) -> None:
+        """Solve every instance from round trip 0 (one persistent launch per grid size)."""
         check(self._lib.cuopo_batch_run(self._h, max_rt, tol, patience, _stream(stream)))
+
+    def reset(self, stream=None) -> None:
+        check(self._lib.cuopo_batch_reset(self._h, _stream(stream)))
+
+    def step(self, chunk: int, max_rt: int, tol: float, patience: int = 1, stream=None) -> None:
+        """Continue every running instance by up to `chunk` round trips."""
+        check(self._lib.cuopo_batch_step(self._h, chunk, max_rt, tol, patience, _stream(stream)))
+
+    def pending(self, stream=None) -> int:
+        n = C.c_int()
+        check(self._lib.cuopo_batch_pending(self._h, C.byref(n), _stream(stream)))
+        return n.value
 
     def results(self, stream=None):
         ps = np.zeros(self.count)

@@ -510,9 +510,10 @@ struct cuopo_batch {
     size_t total;                 /* total signal elements */
     void *d_pump;                 /* pump-field work buffers (n_t per instance) */
     void *d_signal;               /* signal fields, concatenated */
-    double *d_ps;
+    double *d_ps;     /* per-instance resumable state (see Instance::st_*) */
     int *d_rt;
     int *d_flag;
+    int *d_calm;
     std::vector<BatchGroup> groups;
     cudaEvent_t fork;
     std::vector<Instance> h_inst;
@@ -534,6 +535,7 @@ extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
     cudaFree(b->d_ps);
     cudaFree(b->d_rt);
     cudaFree(b->d_flag);
+    cudaFree(b->d_calm);
     delete b;
     return CUOPO_OK;
 }
@@ -573,6 +575,7 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
         (e = cudaMalloc(&b->d_ps, sizeof(double) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rt, sizeof(int) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_flag, sizeof(int) * count)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_calm, sizeof(int) * count)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) {
         cuopo_batch_destroy(b);
         return e == cudaErrorMemoryAllocation ? cuopo_fail(CUOPO_ENOMEM, "batch_create: device allocation failed")
@@ -583,6 +586,7 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
     cudaMemset(b->d_ps, 0, sizeof(double) * count);
     cudaMemset(b->d_rt, 0, sizeof(int) * count);
     cudaMemset(b->d_flag, 0, sizeof(int) * count);
+    cudaMemset(b->d_calm, 0, sizeof(int) * count);
 
     /* one plan (tables) and one persistent launch per distinct grid size */
     std::vector<int> sizes;
@@ -634,9 +638,10 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
             pi.delta = inst[i].delta;
             pi.gdd = inst[i].gdd;
             cavity_factors(pi, I);
-            I.ps_out = b->d_ps + i;
-            I.rt_done = b->d_rt + i;
-            I.flag_out = b->d_flag + i;
+            I.st_ps = b->d_ps + i;
+            I.st_rt = b->d_rt + i;
+            I.st_flag = b->d_flag + i;
+            I.st_calm = b->d_calm + i;
             b->h_inst[i] = I;
         }
         if ((e = cudaMemcpy(g.d_inst, hi.data(), sizeof(Instance) * hi.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
@@ -689,37 +694,64 @@ extern "C" cuopo_status cuopo_batch_get_signal(cuopo_batch *b, void *dst, int on
     return e == cudaSuccess ? CUOPO_OK : cuda_fail(e, "batch_get_signal");
 }
 
-extern "C" cuopo_status cuopo_batch_run(cuopo_batch *b, int max_rt, double tol, int patience, void *stream)
+extern "C" cuopo_status cuopo_batch_reset(cuopo_batch *b, void *stream)
 {
-    if (!b || max_rt < 1) return cuopo_fail(CUOPO_EINVAL, "batch_run: bad argument");
+    if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_reset: NULL batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(b->d_rt, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(b->d_flag, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(b->d_calm, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(b->d_ps, 0, sizeof(double) * b->count, st)) != cudaSuccess)
+        return cuda_fail(e, "batch_reset");
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_step(cuopo_batch *b, int chunk, int max_rt, double tol, int patience,
+                                         void *stream)
+{
+    if (!b || chunk < 1 || max_rt < 1) return cuopo_fail(CUOPO_EINVAL, "batch_step: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaEventRecord(b->fork, st);
-    if (e != cudaSuccess) return cuda_fail(e, "batch_run");
+    if (e != cudaSuccess) return cuda_fail(e, "batch_step");
     for (BatchGroup &g : b->groups) {
-        if ((e = cudaStreamWaitEvent(g.stream, b->fork, 0)) != cudaSuccess) return cuda_fail(e, "batch_run");
-        if ((e = cudaMemsetAsync(g.d_queue, 0, sizeof(int), g.stream)) != cudaSuccess) return cuda_fail(e, "batch_run");
+        if ((e = cudaStreamWaitEvent(g.stream, b->fork, 0)) != cudaSuccess) return cuda_fail(e, "batch_step");
+        if ((e = cudaMemsetAsync(g.d_queue, 0, sizeof(int), g.stream)) != cudaSuccess)
+            return cuda_fail(e, "batch_step");
         LaunchArgs a = base_args(g.plan);
         a.inst = g.d_inst;
         a.n_inst = (int)g.members.size();
         a.queue = g.d_queue;
-        /* rt window, tolerance and patience are per run: patch the descriptors */
-        std::vector<Instance> hi(g.members.size());
-        for (size_t j = 0; j < g.members.size(); j++) {
-            hi[j] = b->h_inst[g.members[j]];
-            hi[j].rt_begin = 0;
-            hi[j].rt_count = max_rt;
-            hi[j].tol = tol;
-            hi[j].patience = patience;
-        }
-        if ((e = cudaMemcpyAsync(g.d_inst, hi.data(), sizeof(Instance) * hi.size(), cudaMemcpyHostToDevice,
-                                 g.stream)) != cudaSuccess)
-            return cuda_fail(e, "batch_run: upload");
-        /* the pageable copy above is staged before the call returns */
+        a.chunk = chunk;
+        a.max_rt = max_rt;
+        a.tol = tol;
+        a.patience = patience;
         cuopo_status s2 = launch(g.plan, a, g.grid, g.stream);
         if (s2 != CUOPO_OK) return s2;
-        if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess) return cuda_fail(e, "batch_run");
-        if ((e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess) return cuda_fail(e, "batch_run");
+        if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess) return cuda_fail(e, "batch_step");
+        if ((e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess) return cuda_fail(e, "batch_step");
     }
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_run(cuopo_batch *b, int max_rt, double tol, int patience, void *stream)
+{
+    cuopo_status st = cuopo_batch_reset(b, stream);
+    if (st != CUOPO_OK) return st;
+    return cuopo_batch_step(b, max_rt, max_rt, tol, patience, stream);
+}
+
+extern "C" cuopo_status cuopo_batch_pending(cuopo_batch *b, int *running, void *stream)
+{
+    if (!b || !running) return cuopo_fail(CUOPO_EINVAL, "batch_pending: NULL argument");
+    std::vector<int> f((size_t)b->count);
+    cudaError_t e = cudaMemcpyAsync(f.data(), b->d_flag, sizeof(int) * b->count, cudaMemcpyDeviceToHost,
+                                    (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch_pending");
+    int n = 0;
+    for (int v : f) n += (v == 0);
+    *running = n;
     return CUOPO_OK;
 }
 

@@ -74,6 +74,13 @@ struct Instance {
     int patience;               /* consecutive rts below tol to stop (>= 1) */
     double *ps_out;             /* final signal power (may be NULL) */
     int *flag_out;              /* 1 converged, 0 max rts reached, 5 non-finite (may be NULL) */
+    /* resumable state of a batch instance (all NULL for single launches):
+     * round trips run so far, last signal power, calm-rt counter and flag
+     * (0 running, 1 converged, 2 round-trip limit reached, 5 non-finite) */
+    int *st_rt;
+    double *st_ps;
+    int *st_calm;
+    int *st_flag;
 };
 
 struct LaunchArgs {
@@ -87,9 +94,13 @@ struct LaunchArgs {
     int pass_only;              /* 1: one crystal pass, no cavity map */
     int use_eom, eom_idler;
     int *status;                /* first error code (atomicCAS from 0) */
+    /* batch launches: continue each running instance by up to `chunk` round
+     * trips, stopping at max_rt; convergence tolerance and patience */
+    int chunk, max_rt, patience;
+    double tol;
 };
 
-enum { ST_OK = 0, ST_NONFINITE = 5 };
+enum { ST_OK = 0, ST_CONVERGED = 1, ST_LIMIT = 2, ST_NONFINITE = 5 };
 
 template <typename C>
 __device__ __forceinline__ C ldc(const void *p, long i)
@@ -359,6 +370,18 @@ struct Ssfm {
             }
             first = false;
             const Instance &I = a.inst ? a.inst[idx] : a.single;
+            int rt_begin = I.rt_begin, rt_count = I.rt_count, patience = I.patience, calm = 0;
+            double tol = I.tol, prev_ps = -1.0;
+            if (I.st_flag) {
+                /* batch instance: resume from its saved state, skip if done */
+                if (*(volatile int *)I.st_flag != 0) continue;
+                rt_begin = *(volatile int *)I.st_rt;
+                rt_count = min(a.chunk, a.max_rt - rt_begin);
+                prev_ps = rt_begin > 0 ? *(volatile double *)I.st_ps : -1.0;
+                calm = *(volatile int *)I.st_calm;
+                tol = a.tol;
+                patience = a.patience;
+            }
 
             C *gf[3] = {reinterpret_cast<C *>(I.Ap), reinterpret_cast<C *>(I.As), reinterpret_cast<C *>(I.Ai)};
 #pragma unroll
@@ -368,11 +391,11 @@ struct Ssfm {
                     home[f * M + swz<C>(t + e * T)] = gf[f][(size_t)rank * M + t + e * T];
             xsync();
 
-            double prev_ps = -1.0, ps = 0.0, acc = 0.0;
-            int rts = 0, calm = 0, flag = 0;
+            double ps = prev_ps, acc = 0.0;
+            int rts = 0, flag = 0;
             bool stop = false;
             const C *last_row = rk + (size_t)(a.n_z - 1) * NCO;
-            for (int rt = I.rt_begin; rt < I.rt_begin + I.rt_count && !stop; rt++) {
+            for (int rt = rt_begin; rt < rt_begin + rt_count && !stop; rt++) {
                 {
                     Ops op{};
                     op.inject = !a.pass_only;
@@ -446,7 +469,7 @@ struct Ssfm {
                     for (int c = 0; c < CL; c++) part += *peer(&red_cl, c);
                 }
                 ps = part * tab.inv_n;
-                if (rank == 0 && t == 0 && I.ps_hist) I.ps_hist[rt - I.rt_begin] = ps;
+                if (rank == 0 && t == 0 && I.ps_hist) I.ps_hist[rt - rt_begin] = ps;
                 if (!(ps == ps) || ps > 1.0e300) {
                     if (rank == 0 && t == 0 && a.status) atomicCAS(a.status, 0, (int)ST_NONFINITE);
                     flag = ST_NONFINITE;
@@ -454,9 +477,9 @@ struct Ssfm {
                 }
                 /* convergence: relative change of the signal power per rt below
                  * tol for `patience` consecutive rts (from the second rt on) */
-                if (I.tol > 0.0 && prev_ps > 0.0 && ps > 0.0 && fabs(ps - prev_ps) < I.tol * ps) {
-                    if (++calm >= (I.patience > 0 ? I.patience : 1) && flag == 0) {
-                        flag = 1;
+                if (tol > 0.0 && prev_ps > 0.0 && ps > 0.0 && fabs(ps - prev_ps) < tol * ps) {
+                    if (++calm >= (patience > 0 ? patience : 1) && flag == 0) {
+                        flag = ST_CONVERGED;
                         stop = true;
                     }
                 } else {
@@ -473,6 +496,12 @@ struct Ssfm {
                 if (I.rt_done) *I.rt_done = rts;
                 if (I.ps_out) *I.ps_out = ps;
                 if (I.flag_out) *I.flag_out = flag;
+                if (I.st_flag) {
+                    *I.st_rt = rt_begin + rts;
+                    *I.st_ps = ps;
+                    *I.st_calm = calm;
+                    *I.st_flag = flag != 0 ? flag : (rt_begin + rts >= a.max_rt ? (int)ST_LIMIT : 0);
+                }
             }
             bar();
         }

@@ -258,12 +258,27 @@ cuopo_status cuopo_batch_set_signal(cuopo_batch *batch, const void *src, int src
 cuopo_status cuopo_batch_get_signal(cuopo_batch *batch, void *dst, int dst_on_device, void *stream);
 /* Runs every instance from round trip 0 until the relative change of its
  * signal power per round trip stays below tol for `patience` consecutive
- * round trips, or max_rt round trips have run.  Asynchronous on stream. */
+ * round trips, or max_rt round trips have run.  Asynchronous on stream.
+ * Equivalent to cuopo_batch_reset + cuopo_batch_step(chunk = max_rt). */
 cuopo_status cuopo_batch_run(cuopo_batch *batch, int max_rt, double tol, int patience, void *stream);
-/* Per-instance final signal power, round trips run and flag (1 converged,
- * 0 round-trip limit, 5 non-finite) into host arrays (any may be NULL).
- * Waits for stream. */
+/* Resumable form: reset every instance to round trip 0 (fields are kept),
+ * then continue every still-running instance by up to `chunk` round trips
+ * per call.  Instance state (round trips run, last power, flag) stays on the
+ * device between calls. */
+cuopo_status cuopo_batch_reset(cuopo_batch *batch, void *stream);
+cuopo_status cuopo_batch_step(cuopo_batch *batch, int chunk, int max_rt, double tol, int patience,
+                              void *stream);
+/* Number of instances still running (synchronous). */
+cuopo_status cuopo_batch_pending(cuopo_batch *batch, int *running, void *stream);
+/* Per-instance last signal power, round trips run and flag (0 running,
+ * 1 converged, 2 round-trip limit reached, 5 non-finite) into host arrays
+ * (any may be NULL).  Waits for stream. */
 cuopo_status cuopo_batch_results(cuopo_batch *batch, double *ps, int *rts, int *flags, void *stream);
+
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 3
+ * launches of an FMA-chain kernel over every SM); the denominator of the
+ * solver's roofline.  Synchronous. */
+cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream);
 
 /* Blocks until the plan's work on stream has finished; returns the first
  * asynchronous error. */
