@@ -16,48 +16,79 @@
  * element-wise work of the solver (RK4, dispersion, cavity map) runs on
  * those registers with no shared-memory exchange or barrier.
  *
- * Twiddles: a radix-16 stage whose sub-transform length is NS needs
- * W^{r k}, W = exp(2 pi i/(16 NS)), k = t mod NS, r = 1..15, fixed per
- * thread for the whole kernel.  Middle stages (NS <= M/256) read them from
- * a small shared-memory table formed in FP64 when the kernel starts
- * (15 NS entries per stage); the last stage (NS = M/16, one set per
- * thread) keeps the six FP64-rounded powers W^{k}, W^{2k}, W^{3k}, W^{4k},
- * W^{8k}, W^{12k} in registers and forms the others as one product
- * W^{4a k} W^{b k}.  Every twiddle is therefore within two roundings of
- * exact.
+ * Twiddles are applied as rotations built from three shears,
+ *   x -= t y;  y += s x;  x -= t y,      t = tan(phi/2), s = sin(phi),
+ * after an exact quarter-turn step (a multiple of i) that leaves
+ * |phi| <= pi/4 (Paeth's three-shear rotation).  Each shear has determinant
+ * exactly 1 whatever the float values of t and s, so a rotation never
+ * changes the power of a field with random phase to first order; a complex
+ * multiplication by float-rounded (cos, sin) does (by |w_f|^2 - 1, a few
+ * 1e-8, systematically), and over the ~10^6 transforms of a long cavity run
+ * that bias moves the steady-state power by ~1e-4.  A radix-16 stage whose
+ * sub-transform length is NS needs W^{r k}, W = exp(2 pi i/(16 NS)),
+ * k = t mod NS: with r = b + 4a it applies the rotation by W^{b k} and then
+ * a rotations by W^{4k}; the four base angles are all below pi/2.  The
+ * last stage keeps its four bases in registers, middle stages read theirs
+ * from a small shared-memory table; both are formed in FP64.
  */
 #pragma once
 #include "cplx.cuh"
 
 namespace cuopo {
 
-/* exp(S * i * pi * K / 8) * x, K compile-time. */
+/* x * i^m (exact). */
+template <int m, typename C>
+__device__ __forceinline__ C iq(C x)
+{
+    constexpr int q = ((m % 4) + 4) % 4;
+    if constexpr (q == 0) return x;
+    else if constexpr (q == 1) return mk<C>(-x.y, x.x);
+    else if constexpr (q == 2) return mk<C>(-x.x, -x.y);
+    else return mk<C>(x.y, -x.x);
+}
+
+template <typename C>
+__device__ __forceinline__ C iq_rt(C x, int m)
+{
+    using R = typename real_of<C>::type;
+    R a = (m & 1) ? -x.y : x.x;
+    R b = (m & 1) ? x.x : x.y;
+    if (m & 2) {
+        a = -a;
+        b = -b;
+    }
+    return mk<C>(a, b);
+}
+
+/* Rotation of x by phi given (t, s) = (tan(phi/2), sin(phi)), three shears. */
+template <typename C, typename R>
+__device__ __forceinline__ C shear_rot(C x, R t, R s)
+{
+    const R x1 = x.x - t * x.y;
+    const R y2 = x.y + s * x1;
+    const R x3 = x1 - t * y2;
+    return mk<C>(x3, y2);
+}
+
+/* exp(S * i * pi * K / 8) * x, K compile-time: quarter turns times a
+ * rotation by r pi / 8, |r| <= 2. */
 template <int S, int K, typename C>
 __device__ __forceinline__ C tw16(C x)
 {
     using R = typename real_of<C>::type;
-    constexpr int k = ((K % 16) + 16) % 16;
-    constexpr double c1 = 0.92387953251128675613;  /* cos(pi/8) */
-    constexpr double s1 = 0.38268343236508977173;  /* sin(pi/8) */
-    constexpr double h = 0.70710678118654752440;   /* sqrt(1/2) */
-    if constexpr (k == 0) return x;
-    else if constexpr (k == 4) return cmul_si<S>(x);
-    else if constexpr (k == 8) return mk<C>(-x.x, -x.y);
-    else if constexpr (k == 12) return cmul_si<-S>(x);
-    else if constexpr (k == 2 || k == 6 || k == 10 || k == 14) {
-        /* (c + i S s) with |c| = |s| = sqrt(1/2) */
-        constexpr double c = (k == 2 || k == 14) ? h : -h;
-        constexpr double s = (k == 2 || k == 6) ? h : -h;
-        constexpr double ss = S * s;
-        /* (a + i b)(c + i ss) */
-        return mk<C>((R)c * x.x - (R)ss * x.y, (R)c * x.y + (R)ss * x.x);
-    } else {
-        constexpr double cs[16] = {1, c1, h, s1, 0, -s1, -h, -c1, -1, -c1, -h, -s1, 0, s1, h, c1};
-        constexpr double sn[16] = {0, s1, h, c1, 1, c1, h, s1, 0, -s1, -h, -c1, -1, -c1, -h, -s1};
-        constexpr double c = cs[k];
-        constexpr double ss = S * sn[k];
-        return mk<C>((R)c * x.x - (R)ss * x.y, (R)c * x.y + (R)ss * x.x);
-    }
+    constexpr int n = S * (((K % 16) + 16) % 16);            /* angle n pi / 8 */
+    constexpr int m = n >= 0 ? (n + 1) / 4 : -((-n + 1) / 4); /* nearest quarter turn */
+    constexpr int r = n - 4 * m;                               /* -1..2 */
+    constexpr double T1 = 0.19891236737965800691;              /* tan(pi/16) */
+    constexpr double S1 = 0.38268343236508977173;              /* sin(pi/8) */
+    constexpr double T2 = 0.41421356237309504880;              /* tan(pi/8) */
+    constexpr double S2 = 0.70710678118654752440;              /* sin(pi/4) */
+    const C y = iq<m>(x);
+    if constexpr (r == 0) return y;
+    else if constexpr (r == 1) return shear_rot(y, (R)T1, (R)S1);
+    else if constexpr (r == -1) return shear_rot(y, (R)-T1, (R)-S1);
+    else if constexpr (r == 2) return shear_rot(y, (R)T2, (R)S2);
+    else return shear_rot(y, (R)-T2, (R)-S2);
 }
 
 template <int S, typename C>
@@ -163,98 +194,85 @@ struct StagePlan {
     }
 };
 
-/* Shared-memory twiddle table of the middle radix-16 stages 1..P-2:
- * entry (p, r, k) = W_{16 NS_p}^{r k}, r = 1..15, k < NS_p. */
+/* Shared-memory table of the middle radix-16 stages 1..P-2: for stage p,
+ * base j = 1..4 and k < NS_p the rotation (tan(theta/2), sin(theta)),
+ * theta = 2 pi j k / (16 NS_p), stored as [p][j][k]. */
 template <int M>
 struct TwTable {
     using SP = StagePlan<M>;
     static constexpr int offset(int p)
     {
         int o = 0;
-        for (int q = 1; q < p; q++) o += 15 * SP::ns(q);
+        for (int q = 1; q < p; q++) o += 4 * SP::ns(q);
         return o;
     }
     static constexpr int size() { return SP::P > 2 ? offset(SP::P - 1) : 0; }
 };
+
+template <typename C>
+__device__ __forceinline__ C rot_params(int jk, int den)
+{
+    using R = typename real_of<C>::type;
+    /* theta = 2 pi jk / den in [0, pi/2): t = tan(theta/2), s = sin(theta) */
+    double sh, ch, sn, cs;
+    sincospi((double)jk / (double)den, &sh, &ch);
+    sincospi(2.0 * (double)jk / (double)den, &sn, &cs);
+    return mk<C>((R)(sh / ch), (R)sn);
+}
 
 /* Fills the table (all threads of the CTA cooperate; caller syncs). */
 template <int M, typename C>
 __device__ __forceinline__ void fill_twiddle_table(C *tab, int t)
 {
     using SP = StagePlan<M>;
-    using R = typename real_of<C>::type;
 #pragma unroll
     for (int p = 1; p + 1 < SP::P; p++) {
         const int ns = SP::ns(p);
         const int off = TwTable<M>::offset(p);
-        for (int idx = t; idx < 15 * ns; idx += SP::T) {
-            const int r = idx / ns + 1, k = idx % ns;
-            double sn, cs;
-            sincospi(2.0 * (double)(r * k) / (16.0 * (double)ns), &sn, &cs);
-            tab[off + idx] = mk<C>((R)cs, (R)sn);
+        for (int idx = t; idx < 4 * ns; idx += SP::T) {
+            const int j = idx / ns + 1, k = idx % ns;
+            tab[off + idx] = rot_params<C>(j * k, 16 * ns);
         }
     }
 }
 
-/* The last radix-16 stage's twiddles of thread t (S = +1 form). */
+/* The last radix-16 stage's four base rotations of thread t. */
 template <int M, typename C>
 struct StageTwiddles {
-    C w1, w2, w3, w4, w8, w12;
-    const C *tab;  /* shared-memory table of the middle stages */
+    C b1, b2, b3, b4;  /* (tan(theta/2), sin(theta)) of W^k, W^2k, W^3k, W^4k */
+    const C *tab;      /* shared-memory table of the middle stages */
     __device__ __forceinline__ void init(int t, const C *table)
     {
-        using R = typename real_of<C>::type;
         using SP = StagePlan<M>;
         tab = table;
         if constexpr (SP::P > 1) {
             const int ns = SP::ns(SP::P - 1);
-            const double k = (double)(t % ns);
-            const double den = 16.0 * (double)ns;
-            double sn, cs;
-            sincospi(2.0 * k / den, &sn, &cs);
-            w1 = mk<C>((R)cs, (R)sn);
-            sincospi(4.0 * k / den, &sn, &cs);
-            w2 = mk<C>((R)cs, (R)sn);
-            sincospi(6.0 * k / den, &sn, &cs);
-            w3 = mk<C>((R)cs, (R)sn);
-            sincospi(8.0 * k / den, &sn, &cs);
-            w4 = mk<C>((R)cs, (R)sn);
-            sincospi(16.0 * k / den, &sn, &cs);
-            w8 = mk<C>((R)cs, (R)sn);
-            sincospi(24.0 * k / den, &sn, &cs);
-            w12 = mk<C>((R)cs, (R)sn);
+            const int k = t % ns;
+            b1 = rot_params<C>(k, 16 * ns);
+            b2 = rot_params<C>(2 * k, 16 * ns);
+            b3 = rot_params<C>(3 * k, 16 * ns);
+            b4 = rot_params<C>(4 * k, 16 * ns);
         }
     }
 };
 
+/* v[4a+b] rotated by S (b k + 4 a k) theta: the rotation by W^{bk}, then a
+ * rotations by W^{4k}. */
 template <int S, typename C>
-__device__ __forceinline__ C cj(C a)
+__device__ __forceinline__ void apply_stage_rotations(C (&v)[16], C b1, C b2, C b3, C b4)
 {
-    return S > 0 ? a : cconj(a);
-}
-
-/* v[4a+b] *= W^{(4a+b)k} from the six register powers (last stage). */
-template <int S, typename C>
-__device__ __forceinline__ void apply_last_twiddles(C (&v)[16], const C &w1, const C &w2, const C &w3,
-                                                    const C &w4, const C &w8, const C &w12)
-{
-    const C b1 = cj<S>(w1), b2 = cj<S>(w2), b3 = cj<S>(w3);
-    const C a1 = cj<S>(w4), a2 = cj<S>(w8), a3 = cj<S>(w12);
-    v[1] = cmul(v[1], b1);
-    v[2] = cmul(v[2], b2);
-    v[3] = cmul(v[3], b3);
-    v[4] = cmul(v[4], a1);
-    v[5] = cmul(v[5], cmul(a1, b1));
-    v[6] = cmul(v[6], cmul(a1, b2));
-    v[7] = cmul(v[7], cmul(a1, b3));
-    v[8] = cmul(v[8], a2);
-    v[9] = cmul(v[9], cmul(a2, b1));
-    v[10] = cmul(v[10], cmul(a2, b2));
-    v[11] = cmul(v[11], cmul(a2, b3));
-    v[12] = cmul(v[12], a3);
-    v[13] = cmul(v[13], cmul(a3, b1));
-    v[14] = cmul(v[14], cmul(a3, b2));
-    v[15] = cmul(v[15], cmul(a3, b3));
+    using R = typename real_of<C>::type;
+    const R sg = (R)S;
+    const C q[4] = {b1, b1, b2, b3};
+#pragma unroll
+    for (int r = 1; r < 16; r++) {
+        const int b = r & 3, a = r >> 2;
+        C x = v[r];
+        if (b) x = shear_rot(x, sg * q[b].x, sg * q[b].y);
+#pragma unroll
+        for (int i = 0; i < a; i++) x = shear_rot(x, sg * b4.x, sg * b4.y);
+        v[r] = x;
+    }
 }
 
 template <int S, int M, int P_IDX, typename C>
@@ -272,12 +290,11 @@ __device__ __forceinline__ void stage_compute(C (&reg)[16], const StageTwiddles<
         if constexpr (NS > 1) {
             static_assert(R == 16, "twiddled stages are radix 16");
             if constexpr (P_IDX + 1 == SP::P) {
-                apply_last_twiddles<S>(v, tw.w1, tw.w2, tw.w3, tw.w4, tw.w8, tw.w12);
+                apply_stage_rotations<S>(v, tw.b1, tw.b2, tw.b3, tw.b4);
             } else {
                 const int k = threadIdx.x % NS;
                 const C *row = tw.tab + TwTable<M>::offset(P_IDX) + k;
-#pragma unroll
-                for (int r = 1; r < 16; r++) v[r] = cmul(v[r], cj<S>(row[(r - 1) * NS]));
+                apply_stage_rotations<S>(v, row[0], row[NS], row[2 * NS], row[3 * NS]);
             }
         }
         dft<S, R>(v);

@@ -30,6 +30,8 @@ struct cuopo_plan {
     void *d_eom;      /* [N] or NULL */
     float *d_w;       /* [CL][M], same permutation */
     void *d_twN;      /* [N] W_N^q (cluster plans) or NULL */
+    double2 *d_frame_u; /* [NFRAME] random frame angles */
+    void *d_frame_c;    /* [NFRAME][3] their phasors */
     int *d_status;
     double h6;
 };
@@ -201,8 +203,8 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
     const int N = p.n_t;
     const int F = p.n_eqs;
     /* LinearOperator, cwes2.cuh:103-121 / cwes3.cuh:107-128: per field the
-     * group-velocity term (Q4), GVD, TOD, attenuation exp(-alpha dz/2),
-     * and CUFFTscale's 1/N (functions.cuh:126-135). */
+     * group-velocity term (Q4), GVD, TOD, attenuation exp(-alpha dz/2);
+     * CUFFTscale's 1/N (functions.cuh:126-135) is applied in the kernel. */
     double gvm[3], b2[3], b3[3], al[3];
     if (F == 2) {
         gvm[0] = 1.0 / p.vp - 1.0 / p.vs;
@@ -224,19 +226,28 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
         for (int k = 0; k < N; k++) {
             const double wk = (double)w[k];
             const double ph = z * wk * (gvm[f] + 0.5 * wk * b2[f] + wk * wk * b3[f] / 6.0);
-            /* frequency k = k2 + CL k1 is entry k1 of CTA k2's row */
+            /* frequency k = k2 + CL k1 is entry k1 of CTA k2's row.  Stored as
+             * d = N D - 1 and applied as (A + A d) / N: the factor's float
+             * rounding error then scales with |d| (tiny near w = 0, where CW
+             * fields live) instead of biasing every slice by up to half an
+             * ulp of att, which would compound over thousands of round trips. */
             const int k2 = k % CL, k1 = k / CL;
-            D[(size_t)f * N + (size_t)k2 * M + k1] = mk<C>((R)(std::cos(ph) * att), (R)(std::sin(ph) * att));
+            const double a = att * (double)N;
+            const double dre = (ph == 0.0) ? a - 1.0 : a * std::cos(ph) - 1.0;
+            D[(size_t)f * N + (size_t)k2 * M + k1] = mk<C>((R)dre, (R)(a * std::sin(ph)));
         }
     }
-    /* cross-stage twiddles W_N^q = exp(2 pi i q / N) */
+    /* cross-stage twiddles W_N^q = exp(2 pi i q / N) as a quarter turn
+     * m = round(4q/N) (recomputed in the kernel) and the residual rotation
+     * phi = 2 pi q/N - m pi/2, |phi| <= pi/4, stored as (tan(phi/2), sin(phi)) */
     twn_out.clear();
     if (CL > 1) {
         twn_out.resize(sizeof(C) * (size_t)N);
         C *W = reinterpret_cast<C *>(twn_out.data());
-        for (int q = 0; q < N; q++) {
-            const double a = 2.0 * M_PI * (double)q / (double)N;
-            W[q] = mk<C>((R)std::cos(a), (R)std::sin(a));
+        for (long q = 0; q < N; q++) {
+            const long m = (4 * q + N / 2) / N;
+            const double phi = 2.0 * M_PI * (double)(4 * q - m * N) / (4.0 * (double)N);
+            W[q] = mk<C>((R)std::tan(0.5 * phi), (R)std::sin(phi));
         }
     }
     /* RK4 stage coefficients per slice (one extra zero row at the end). */
@@ -351,6 +362,41 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
         cuopo_plan_destroy(pl);
         return cuda_fail(e, "plan_create: upload");
     }
+    {
+        /* random frame table: u_s, u_i uniform in [0,1) turns (fixed seed) */
+        std::vector<double2> fu(NFRAME);
+        const size_t csz = precision == CUOPO_F32 ? sizeof(float2) : sizeof(double2);
+        std::vector<unsigned char> fc(csz * 3 * NFRAME);
+        unsigned long long st = 0x2545F4914F6CDD1Dull;
+        auto next = [&st]() {
+            st += 0x9E3779B97F4A7C15ull;
+            unsigned long long z = st;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            return (double)((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+        };
+        for (int q = 0; q < NFRAME; q++) {
+            /* frame angles in [-1/8, 1/8) turns; the pump turns by their sum,
+             * at most a quarter turn, so no quarter-turn step is needed */
+            const double us = 0.25 * next() - 0.125, ui = 0.25 * next() - 0.125;
+            fu[q] = make_double2(us, ui);
+            const double up = (p->n_eqs == 2) ? 2.0 * us : us + ui;
+            const double ang[3] = {2.0 * M_PI * up, 2.0 * M_PI * us, 2.0 * M_PI * ui};
+            for (int f = 0; f < 3; f++) {
+                const double tt = std::tan(0.5 * ang[f]), ss = std::sin(ang[f]);
+                if (precision == CUOPO_F32) ((float2 *)fc.data())[3 * q + f] = make_float2((float)tt, (float)ss);
+                else ((double2 *)fc.data())[3 * q + f] = make_double2(tt, ss);
+            }
+        }
+        if ((e = cudaMalloc(&pl->d_frame_u, sizeof(double2) * NFRAME)) != cudaSuccess ||
+            (e = cudaMalloc(&pl->d_frame_c, fc.size())) != cudaSuccess ||
+            (e = cudaMemcpy(pl->d_frame_u, fu.data(), sizeof(double2) * NFRAME, cudaMemcpyHostToDevice)) !=
+                cudaSuccess ||
+            (e = cudaMemcpy(pl->d_frame_c, fc.data(), fc.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            cuopo_plan_destroy(pl);
+            return cuda_fail(e, "plan_create: frame table");
+        }
+    }
     *out = pl;
     return CUOPO_OK;
 }
@@ -363,6 +409,8 @@ extern "C" cuopo_status cuopo_plan_destroy(cuopo_plan *pl)
     cudaFree(pl->d_eom);
     cudaFree(pl->d_w);
     cudaFree(pl->d_twN);
+    cudaFree(pl->d_frame_u);
+    cudaFree(pl->d_frame_c);
     cudaFree(pl->d_status);
     delete pl;
     return CUOPO_OK;
@@ -386,6 +434,8 @@ static LaunchArgs base_args(const cuopo_plan *pl)
     a.tab.eom = pl->d_eom;
     a.tab.w = pl->d_w;
     a.tab.twN = pl->d_twN;
+    a.tab.frame_u = pl->d_frame_u;
+    a.tab.frame_c = pl->d_frame_c;
     a.tab.h6 = pl->h6;
     a.tab.inv_n = 1.0 / (double)pl->N;
     a.n_z = pl->p.n_z;

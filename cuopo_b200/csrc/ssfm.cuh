@@ -50,6 +50,8 @@ struct Tables {
     const void *eom;    /* [N]: exp(i m sin(2 pi fpm T)) or NULL */
     const float *w;     /* [CL][M]: angular frequency grid (reference float values) */
     const void *twN;    /* [N]: W_N^q (cross-stage twiddles; CL > 1) */
+    const double2 *frame_u; /* [NFRAME]: random frame angles (u_s, u_i) in turns, |u| < 1/8 */
+    const void *frame_c;    /* [NFRAME][3]: rotation (tan, sin) for pump, signal, idler */
     double h6;          /* (dz/2)/6 */
     double inv_n;       /* 1/N */
 };
@@ -101,6 +103,25 @@ struct LaunchArgs {
 };
 
 enum { ST_OK = 0, ST_CONVERGED = 1, ST_LIMIT = 2, ST_NONFINITE = 5 };
+
+/* Random frame rotations.  The coupled-wave equations are invariant under
+ * (Ap, As, Ai) -> (Ap e^{i(a+b)}, As e^{ia}, Ai e^{ib}) (and Ap e^{2ia} in the
+ * degenerate 2-equation model), and the linear steps commute with it.  Each
+ * slice the kernel moves the fields to a new frame drawn from a fixed table
+ * and returns them to the laboratory frame before the cavity map; the
+ * rounding errors of the float transforms then have random phase relative
+ * to the field, so they do not add up coherently over the ~10^5 slices of a
+ * run.  Entry of slice s of round trip rt: frame_index(rt, s). */
+enum { NFRAME = 1024 };
+
+__host__ __device__ __forceinline__ int frame_index(int rt, int s)
+{
+    unsigned long long z = ((unsigned long long)(unsigned)rt << 32) ^ (unsigned)s ^ 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (int)(z & (NFRAME - 1));
+}
 
 template <typename C>
 __device__ __forceinline__ C ldc(const void *p, long i)
@@ -171,12 +192,50 @@ struct Ssfm {
         long poff;          /* NS pump window offset of this round trip */
         const C *rk0, *rk1; /* RK4 half steps to apply (NULL: none) */
         int eom;            /* intracavity phase modulator */
+        int rotate;         /* frame rotation: quarter turns rq[f], then the shear rotation rf[f] */
+        C rf[3];
+        int rq[3];
         int addphase;       /* AddPhase on the resonant fields */
-        C ph_s, ph_i;
+        double2 ph_s, ph_i;
         int save;           /* SaveRoundTrip into slot */
         size_t slot;
         int power;          /* accumulate |As|^2 */
     };
+
+    /* Move to the frame of table entry q (rotation by 2 pi u per field, built
+     * from shears); th accumulates each field's frame angle in turns. */
+    static __device__ __forceinline__ void frame_step(Ops &op, const Tables &tab, int q, double (&th)[3])
+    {
+        const C *fc = reinterpret_cast<const C *>(tab.frame_c) + 3 * q;
+        const double2 u = tab.frame_u[q];
+        op.rotate = 1;
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            op.rf[f] = fc[f];
+            op.rq[f] = 0;
+        }
+        th[1] += u.x;
+        th[2] += u.y;
+        th[0] += (F == 2) ? 2.0 * u.x : u.x + u.y;
+    }
+
+    /* Back to the laboratory frame: rotation by -th = quarter turns plus a
+     * residual of at most 1/8 turn, formed in FP64. */
+    static __device__ __forceinline__ void frame_back(Ops &op, const double (&th)[3])
+    {
+        op.rotate = 1;
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            const double back = -th[f];
+            const double qt = rint(4.0 * back);
+            const double res = back - 0.25 * qt; /* turns, |res| <= 1/8 */
+            double sh, ch, sn, cs;
+            sincospi(res, &sh, &ch);
+            sincospi(2.0 * res, &sn, &cs);
+            op.rq[f] = ((int)fmod(qt, 4.0) + 4) & 3;
+            op.rf[f] = mk<C>((R)(sh / ch), (R)sn);
+        }
+    }
 
     static __device__ __forceinline__ void xsync()
     {
@@ -196,6 +255,13 @@ struct Ssfm {
         else return cg::this_cluster().map_shared_rank(p, rank);
     }
 
+    static __device__ __forceinline__ C mul_fp64(C a, double2 f)
+    {
+        const double re = (double)a.x * f.x - (double)a.y * f.y;
+        const double im = (double)a.x * f.y + (double)a.y * f.x;
+        return mk<C>((R)re, (R)im);
+    }
+
     static __device__ __forceinline__ void pointwise(C (&A)[3], int n, const Ops &op, const Instance &I,
                                                      const Tables &tab, R h6, int eom_idler, double &acc)
     {
@@ -213,9 +279,15 @@ struct Ssfm {
             A[1] = cmul(A[1], ef);
             if (F == 3 && eom_idler) A[F - 1] = cmul(A[F - 1], ef);
         }
+        if (op.rotate) {
+#pragma unroll
+            for (int f = 0; f < F; f++) A[f] = shear_rot(iq_rt(A[f], op.rq[f]), op.rf[f].x, op.rf[f].y);
+        }
         if (op.addphase) {
-            A[1] = cmul(A[1], op.ph_s);
-            if constexpr (F == 3) A[2] = cmul(A[2], op.ph_i);
+            /* in FP64 so that sqrt(R) exp(i pi delta) carries no float rounding
+             * bias into the round-trip gain */
+            A[1] = mul_fp64(A[1], op.ph_s);
+            if constexpr (F == 3) A[2] = mul_fp64(A[2], op.ph_i);
         }
         if (op.save) {
             C *sv[3] = {reinterpret_cast<C *>(I.sv_p), reinterpret_cast<C *>(I.sv_s),
@@ -248,15 +320,23 @@ struct Ssfm {
 #pragma unroll
                 for (int f = 0; f < F; f++) v[f][c] = src[f * M + sm];
             }
+            /* cross-stage twiddles W_N^{n1 c}: quarter turn m and the residual
+             * rotation (tan, sin) from the table */
             C w[CL];
+            int qm[CL];
             if constexpr (CL > 1) {
 #pragma unroll
-                for (int c = 1; c < CL; c++) w[c] = __ldg(twN + (long)n1 * c);
+                for (int c = 1; c < CL; c++) {
+                    const long q = (long)n1 * c;
+                    w[c] = __ldg(twN + q);
+                    qm[c] = (int)(((4 * q + N / 2) / N) & 3);
+                }
 #pragma unroll
                 for (int f = 0; f < F; f++) {
                     if ((in_y >> f) & 1u) {
 #pragma unroll
-                        for (int c = 1; c < CL; c++) v[f][c] = cmulc(v[f][c], w[c]);
+                        for (int c = 1; c < CL; c++)
+                            v[f][c] = shear_rot(iq_rt(v[f][c], (-qm[c]) & 3), -w[c].x, -w[c].y);
                         dft<-1, CL>(v[f]);
                     }
                 }
@@ -276,7 +356,7 @@ struct Ssfm {
                     if ((out_y >> f) & 1u) {
                         dft<+1, CL>(v[f]);
 #pragma unroll
-                        for (int c = 1; c < CL; c++) v[f][c] = cmul(v[f][c], w[c]);
+                        for (int c = 1; c < CL; c++) v[f][c] = shear_rot(iq_rt(v[f][c], qm[c]), w[c].x, w[c].y);
                     }
                 }
             }
@@ -301,18 +381,26 @@ struct Ssfm {
         C *bufA = INPLACE ? home : scratch;
         C *bufB = home;
         local_transform<+1, M, 0, INPLACE>(reg, bufA, bufB, tw, t);
+        /* the factor F = 1 + d is applied as (A + A d) / N (1/N is exact) */
+        const R s_n = (R)inv_n;
         if constexpr (MODE == 0) {
 #pragma unroll
-            for (int e = 0; e < 16; e++) reg[e] = cmul(reg[e], __ldg(row + t + e * T));
+            for (int e = 0; e < 16; e++) {
+                const C x = cscale(reg[e], s_n);
+                reg[e] = cadd(x, cmul(x, __ldg(row + t + e * T)));
+            }
         } else {
 #pragma unroll 4
             for (int e = 0; e < 16; e++) {
-                /* functions.cuh:156-186 with CUFFTscale folded in */
+                /* functions.cuh:156-186, formed in FP64 */
                 const double wk = (double)__ldg(w + t + e * T);
                 const double ph = use_tod ? 0.5 * wk * (wk * gdd + wk * wk * tod / 3.0) : 0.5 * wk * wk * gdd;
                 double sn, cs;
                 sincos(ph, &sn, &cs);
-                reg[e] = cmul(reg[e], mk<C>((R)(cs * inv_n), (R)(sn * inv_n)));
+                /* cos(ph) - 1 = -2 sin^2(ph/2), exact for small ph */
+                const double sh = sin(0.5 * ph);
+                const C x = cscale(reg[e], s_n);
+                reg[e] = cadd(x, cmul(x, mk<C>((R)(-2.0 * sh * sh), (R)sn)));
             }
         }
         local_transform<-1, M, P - 1, INPLACE>(reg, bufA, bufB, tw, t);
@@ -396,6 +484,7 @@ struct Ssfm {
             bool stop = false;
             const C *last_row = rk + (size_t)(a.n_z - 1) * NCO;
             for (int rt = rt_begin; rt < rt_begin + rt_count && !stop; rt++) {
+                double th[3] = {0.0, 0.0, 0.0};
                 {
                     Ops op{};
                     op.inject = !a.pass_only;
@@ -405,6 +494,7 @@ struct Ssfm {
                         op.poff = (rt == 0) ? 0 : ((rt > 0 && rt < nrt - 1) ? (long)rt * N : (long)N * nrt - 1 - N);
                     }
                     op.rk0 = rk;
+                    frame_step(op, tab, frame_index(rt, 0), th);
                     cross(home, 0u, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
                 }
@@ -412,12 +502,13 @@ struct Ssfm {
 #pragma unroll 1
                     for (int f = 0; f < F; f++)
                         spectral<0>(home + f * M, scratch, disp + ((size_t)f * CL + rank) * M, nullptr, 0.0, 0.0,
-                                    0, 0.0, tw, t);
+                                    0, tab.inv_n, tw, t);
                     xsync();
                     if (s + 1 < a.n_z) {
                         Ops op{};
                         op.rk0 = rk + (size_t)s * NCO;
                         op.rk1 = rk + (size_t)(s + 1) * NCO;
+                        frame_step(op, tab, frame_index(rt, s + 1), th);
                         cross(home, ALL, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
                         xsync();
                     }
@@ -426,6 +517,7 @@ struct Ssfm {
                 if (a.pass_only) {
                     Ops op{};
                     op.rk0 = last_row;
+                    frame_back(op, th);
                     cross(home, ALL, 0u, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
                     break;
@@ -433,8 +525,8 @@ struct Ssfm {
                 const bool save = (rt >= I.save_first && rt < I.save_first + I.save_count);
                 Ops end{};
                 end.addphase = 1;
-                end.ph_s = mk<C>((R)I.phase_s[0], (R)I.phase_s[1]);
-                end.ph_i = mk<C>((R)I.phase_i[0], (R)I.phase_i[1]);
+                end.ph_s = make_double2(I.phase_s[0], I.phase_s[1]);
+                end.ph_i = make_double2(I.phase_i[0], I.phase_i[1]);
                 end.save = save;
                 end.slot = save ? (size_t)(rt - I.save_first) * N : 0;
                 end.power = 1;
@@ -453,10 +545,12 @@ struct Ssfm {
                         spectral<1>(home + 2 * M, scratch, nullptr, wtab, I.gdd, I.tod_i, I.use_tod_i, tab.inv_n, tw,
                                     t);
                     xsync();
+                    frame_back(end, th);
                     cross(home, res, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 } else {
                     end.rk0 = last_row;
                     end.eom = a.use_eom;
+                    frame_back(end, th);
                     cross(home, ALL, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 }
                 /* signal power over the cluster, summed in rank order by every CTA */
