@@ -113,6 +113,7 @@ SIGNATURES = {
     "cuopo_batch_pending": (_i, [_vp, C.POINTER(_i), _vp]),
     "cuopo_batch_results": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cuopo_probe_fp32_peak": (_i, [C.POINTER(_d), _vp]),
+    "cuopo_crystal_pass_noalloc": (_i, [C.POINTER(Params), _vp, _vp, _vp, _vp, _vp]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

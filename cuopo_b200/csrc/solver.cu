@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "cuopo.h"
@@ -818,5 +819,178 @@ extern "C" cuopo_status cuopo_batch_results(cuopo_batch *b, double *ps, int *rts
         (e = cudaMemcpyAsync(flags, b->d_flag, sizeof(int) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "batch_results");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch_results");
+    return CUOPO_OK;
+}
+
+/* ------------------------------------------------- allocation-free pass */
+
+/*
+ * cuopo_crystal_pass_noalloc: one crystal pass for callers that must not
+ * allocate device memory -- code running while a CUDA graph is being
+ * captured, processes whose device memory is owned by another allocator or
+ * budget, or plugins loaded into such processes.  Its tables live in the
+ * file-scope array below (every GPU that loads the library holds it until
+ * exit); the host side builds them in a static host buffer and uploads them
+ * with cudaMemcpyAsync.  The array is shared by every call, so calls that
+ * overlap on the GPU (different streams, or different host threads without
+ * ordering) race; calls ordered on one stream do not.
+ */
+#define CUOPO_NOALLOC_BYTES (384u * 1024u)
+#define CUOPO_NOALLOC_MAX_N 8192
+#define CUOPO_NOALLOC_MAX_NZ 1024
+#define CUOPO_NOALLOC_MAX_DEV 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CUOPO_NOALLOC_BYTES];
+static unsigned char g_noalloc_host[CUOPO_NOALLOC_BYTES];
+static void *g_noalloc_dev[CUOPO_NOALLOC_MAX_DEV];
+static std::mutex g_noalloc_mu;
+
+extern "C" cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const float *w_host, void *Ap, void *As,
+                                                   void *Ai, void *stream)
+{
+    if (!p || !Ap || !As || (p->n_eqs == 3 && !Ai)) return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: NULL argument");
+    if (p->n_eqs != 2 && p->n_eqs != 3) return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: n_eqs must be 2 or 3");
+    if (!is_pow2i(p->n_t) || p->n_t < 512 || p->n_t > CUOPO_NOALLOC_MAX_N)
+        return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: n_t must be a power of 2 in [512, 8192] "
+                                        "(its tables live in a fixed 384 KiB device array)");
+    if (p->n_z < 1 || p->n_z > CUOPO_NOALLOC_MAX_NZ)
+        return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: n_z must be in [1, 1024]");
+    const KernelEntry *k = find_kernel(CUOPO_F32, p->n_eqs, p->n_t);
+    if (!k || k->CL != 1) return cuopo_fail(CUOPO_EUNSUPPORTED, "crystal_pass_noalloc: no single-CTA kernel for n_t");
+    const int N = p->n_t, F = p->n_eqs, nco = (F == 2) ? 6 : 3;
+
+    /* layout of the scratch array (bytes, 256-aligned pieces) */
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_disp = 0;
+    const size_t o_rk = o_disp + up(sizeof(float2) * (size_t)F * N);
+    const size_t o_w = o_rk + up(sizeof(float2) * (size_t)(p->n_z + 1) * nco);
+    const size_t o_fu = o_w + up(sizeof(float) * (size_t)N);
+    const size_t o_fc = o_fu + up(sizeof(double2) * NFRAME);
+    const size_t o_st = o_fc + up(sizeof(float2) * 3 * NFRAME);
+    const size_t total = o_st + 256;
+    if (total > CUOPO_NOALLOC_BYTES) return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: tables exceed 384 KiB");
+
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "crystal_pass_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= CUOPO_NOALLOC_MAX_DEV) return cuopo_fail(CUOPO_EUNSUPPORTED, "crystal_pass_noalloc: device index");
+    if (!g_noalloc_dev[dev]) {
+        /* once per device, with that device current: the array's device address */
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return cuda_fail(e, "crystal_pass_noalloc: cudaGetSymbolAddress");
+        g_noalloc_dev[dev] = ptr;
+    }
+    unsigned char *H = g_noalloc_host;
+    unsigned char *D = (unsigned char *)g_noalloc_dev[dev];
+
+    /* grid w (reference linspace/fftshift unless given) */
+    float *w = (float *)(H + o_w);
+    if (w_host) std::memcpy(w, w_host, sizeof(float) * N);
+    else {
+        if (p->t_rt <= 0) return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: t_rt must be > 0 when w is not given");
+        /* cuOPO.cu:151,183-189 without a temporary: F[i] = linspace(-N dF/2, N dF/2), w = 2 pi fftshift(F) */
+        const float trt = (float)p->t_rt, dF = 1 / trt;
+        const float lo = (float)(-0.5 * (double)(unsigned)N * (double)dF);
+        const float hi = (float)(+0.5 * (double)(unsigned)N * (double)dF);
+        const float span = hi - lo, den = (float)(N - 1);
+        const float twopi = 2 * (float)3.14159265358979323846;
+        for (int i = 0; i < N; i++) {
+            const int src = (i < N / 2) ? i + N / 2 : i - N / 2;
+            w[i] = twopi * (lo + (float)src * span / den);
+        }
+    }
+    /* dispersion rows (1 + d form), as in the plan's tables */
+    float2 *Dt = (float2 *)(H + o_disp);
+    double gvm[3], b2[3], b3[3], al[3];
+    if (F == 2) { gvm[0] = 1.0 / p->vp - 1.0 / p->vs; gvm[1] = 0.0; }
+    else { gvm[0] = 1.0 / p->vp - 1.0 / p->vi; gvm[1] = 0.0; gvm[2] = 1.0 / p->vi - 1.0 / p->vs; }
+    b2[0] = p->b2p; b2[1] = p->b2s; b2[2] = p->b2i;
+    b3[0] = p->b3p; b3[1] = p->b3s; b3[2] = p->b3i;
+    al[0] = p->alpha_crp; al[1] = p->alpha_crs; al[2] = p->alpha_cri;
+    for (int f = 0; f < F; f++) {
+        const double a = std::exp(-0.5 * al[f] * p->dz);
+        for (int q = 0; q < N; q++) {
+            const double wk = (double)w[q];
+            const double ph = p->dz * wk * (gvm[f] + 0.5 * wk * b2[f] + wk * wk * b3[f] / 6.0);
+            const double dre = (ph == 0.0) ? a - 1.0 : a * std::cos(ph) - 1.0;
+            Dt[(size_t)f * N + q] = make_float2((float)dre, (float)(a * std::sin(ph)));
+        }
+    }
+    /* RK4 stage coefficients (z accumulated in float, as the reference) */
+    float2 *co = (float2 *)(H + o_rk);
+    std::memset(co, 0, sizeof(float2) * (size_t)(p->n_z + 1) * nco);
+    const double h6 = (double)(float)((float)p->dz / 2) / 6.0;
+    float z = 0;
+    const float dzf = (float)p->dz;
+    for (int s = 0; s < p->n_z; s++) {
+        const double zj[3] = {(double)z, (double)(float)(z + dzf / 4), (double)(float)(z + dzf / 2)};
+        if (F == 2) {
+            for (int j = 0; j < 3; j++) {
+                const double ph = p->dk * zj[j], c = std::cos(ph), sn = std::sin(ph);
+                co[s * 6 + 2 * j + 0] = make_float2((float)(-p->kp * sn), (float)(p->kp * c));
+                co[s * 6 + 2 * j + 1] = make_float2((float)(p->ks * sn), (float)(p->ks * c));
+            }
+        } else {
+            double er = 0, ei = 0;
+            const double wgt[3] = {1.0, 4.0, 1.0};
+            for (int j = 0; j < 3; j++) {
+                er += wgt[j] * std::cos(p->dk * zj[j]);
+                ei += wgt[j] * std::sin(p->dk * zj[j]);
+            }
+            const double kap[3] = {p->kp, p->ks, p->ki};
+            for (int f = 0; f < 3; f++) {
+                const double si = (f == 0) ? -ei : ei;
+                co[s * 3 + f] = make_float2((float)(h6 * kap[f] * -si), (float)(h6 * kap[f] * er));
+            }
+        }
+        z += dzf;
+    }
+    /* random frame table (same fixed sequence as the plans') */
+    double2 *fu = (double2 *)(H + o_fu);
+    float2 *fc = (float2 *)(H + o_fc);
+    unsigned long long rs = 0x2545F4914F6CDD1Dull;
+    for (int q = 0; q < NFRAME; q++) {
+        double u[2];
+        for (int j = 0; j < 2; j++) {
+            rs += 0x9E3779B97F4A7C15ull;
+            unsigned long long x = rs;
+            x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+            x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+            u[j] = 0.25 * ((double)((x ^ (x >> 31)) >> 11) * (1.0 / 9007199254740992.0)) - 0.125;
+        }
+        fu[q] = make_double2(u[0], u[1]);
+        const double upump = (F == 2) ? 2.0 * u[0] : u[0] + u[1];
+        const double ang[3] = {2.0 * M_PI * upump, 2.0 * M_PI * u[0], 2.0 * M_PI * u[1]};
+        for (int f = 0; f < 3; f++) fc[3 * q + f] = make_float2((float)std::tan(0.5 * ang[f]), (float)std::sin(ang[f]));
+    }
+
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((e = cudaMemcpyAsync(D, H, o_st, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(D + o_st, 0, sizeof(int), st)) != cudaSuccess)
+        return cuda_fail(e, "crystal_pass_noalloc: table upload");
+
+    LaunchArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.tab.disp = D + o_disp;
+    a.tab.rk = D + o_rk;
+    a.tab.eom = nullptr;
+    a.tab.w = (const float *)(D + o_w);
+    a.tab.twN = nullptr;
+    a.tab.frame_u = (const double2 *)(D + o_fu);
+    a.tab.frame_c = D + o_fc;
+    a.tab.h6 = h6;
+    a.tab.inv_n = 1.0 / (double)N;
+    a.n_z = p->n_z;
+    a.regime = p->regime;
+    a.pass_only = 1;
+    a.status = (int *)(D + o_st);
+    a.single.Ap = Ap;
+    a.single.As = As;
+    a.single.Ai = Ai;
+    a.single.rt_count = 1;
+    e = k->fn(a, 1, st);
+    if (e != cudaSuccess) return cuda_fail(e, "crystal_pass_noalloc: kernel launch");
     return CUOPO_OK;
 }

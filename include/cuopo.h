@@ -275,6 +275,24 @@ cuopo_status cuopo_batch_pending(cuopo_batch *batch, int *running, void *stream)
  * (any may be NULL).  Waits for stream. */
 cuopo_status cuopo_batch_results(cuopo_batch *batch, double *ps, int *rts, int *flags, void *stream);
 
+/*
+ * One crystal pass that allocates no device memory, for callers that cannot
+ * call cudaMalloc: code running while a CUDA graph is being captured, or a
+ * plugin in a process whose device memory belongs to another allocator.  It
+ * has no counterpart in the reference (whose caller allocates every buffer,
+ * src/cuOPO.cu:384-442).  Same computation as cuopo_crystal_pass on an FP32
+ * plan built from (p, w_host); fields are float pairs (device).  Its tables
+ * are written into a fixed 384 KiB device array inside this library (held
+ * by every GPU that loads it until exit), so n_t must be a power of 2 in
+ * [512, 8192] and n_z in [1, 1024]; larger sizes return CUOPO_EINVAL.  The
+ * first call on a device looks up that array's address (make it before any
+ * stream capture); the array is shared by all calls, so calls that overlap
+ * on the GPU race -- order them on one stream.  w_host: the n_t angular
+ * frequencies, or NULL to build them from p->t_rt.
+ */
+cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const float *w_host, void *Ap, void *As,
+                                        void *Ai, void *stream);
+
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 3
  * launches of an FMA-chain kernel over every SM); the denominator of the
  * solver's roofline.  Synchronous. */
