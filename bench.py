@@ -66,7 +66,12 @@ def parse():
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--no-validate", action="store_true", help="skip the FP64 check of converged instances")
     ap.add_argument("--record", type=str, default="", help="write per-instance round trips to this file")
-    return ap.parse_args()
+    ap.add_argument("--sizes", type=str, default="", help="grid sizes to draw from (default 4096,8192,16384,32768); "
+                    "reduced variants are for profiling only")
+    ap.add_argument("--max-rt", type=int, default=MAX_RT, help="round-trip limit (default 5000)")
+    a = ap.parse_args()
+    a.sizes = tuple(int(x) for x in a.sizes.split(",")) if a.sizes else SIZES
+    return a
 
 
 def flops_per_instance_rt(n_t: int, gdd: float) -> float:
@@ -247,11 +252,12 @@ def run_cuopo(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from cuopo_b200 import sweep
-    base, insts, table = sweep.random_cw_sweep(args.count, rank, n_t_choices=SIZES, n_z=N_Z)
-    wbase, winsts, _ = sweep.random_cw_sweep(args.count, 10_000 + rank, n_t_choices=SIZES, n_z=N_Z)
-    rec = load_rts_record(args.count)
+    max_rt = args.max_rt
+    base, insts, table = sweep.random_cw_sweep(args.count, rank, n_t_choices=args.sizes, n_z=N_Z)
+    wbase, winsts, _ = sweep.random_cw_sweep(args.count, 10_000 + rank, n_t_choices=args.sizes, n_z=N_Z)
+    rec = load_rts_record(args.count) if args.sizes == SIZES and max_rt == MAX_RT else None
     cpu = None
-    if rank == 0:  # before any GPU work
+    if rank == 0 and args.sizes == SIZES:  # before any GPU work
         cpu = cpu_baseline_leg(insts, rts_by_size_from(rec, table) if rec else
                                {n: MAX_RT * int(np.sum(table["n_t"] == n)) for n in SIZES})
 
@@ -283,12 +289,12 @@ def run_cuopo(args):
     h_res = np.zeros((3, args.count))
 
     K = max(1, args.steps)
-    chunk = int(math.ceil(MAX_RT / K))
+    chunk = int(math.ceil(max_rt / K))
     # warm-up: the same kind of step on the warm-up sweep
     warm.set_signal(w_init)
     warm.reset()
     for _ in range(max(0, args.warmup)):
-        warm.step(chunk, MAX_RT, TOL, 1)
+        warm.step(chunk, max_rt, TOL, 1)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -306,7 +312,7 @@ def run_cuopo(args):
     e_h2d.record(stream)
     for k in range(K):
         ks[k][0].record(stream)
-        batch.step(chunk, MAX_RT, TOL, 1)
+        batch.step(chunk, max_rt, TOL, 1)
         ks[k][1].record(stream)
     ps, rts, flags = batch.results()   # device -> host (synchronises the stream)
     batch.get_signal(h_out)
@@ -349,7 +355,9 @@ def run_cuopo(args):
 
     traffic = None
     if TRAFFIC_RECORD.exists():
-        traffic = json.loads(TRAFFIC_RECORD.read_text()).get("dram_bytes_per_step_scaled")
+        # DRAM bytes per instance-point and launch from one ncu capture; a step is one launch per grid size
+        rate = json.loads(TRAFFIC_RECORD.read_text()).get("dram_bytes_per_instance_point")
+        traffic = rate * float(np.sum(nt_o)) if rate else None
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -368,6 +376,7 @@ def run_cuopo(args):
                                    "N~U[1.2,6], delta~U[-pi,pi] rad, GDD~U[-500,500] fs^2, R~U[0.90,0.99], "
                                    "grid 2^12..2^15, 100 slices/pass, tol 1e-7, max 5000 rt, noise 1e-15",
                        "global_batch": args.count * world, "per_rank_batch": args.count,
+                       "grid_sizes": list(args.sizes), "max_rt": max_rt,
                        "round_trips_per_step": chunk, "parallelism": f"instances sharded, {world} rank(s)",
                        "l2": "working set (fields of 1024 instances, 252 MB) larger than L2",
                        "solves_converged": conv_all, "solves_total": done_all,
@@ -377,6 +386,7 @@ def run_cuopo(args):
             "hbm_frac": (hbm_bytes / (dev_ms * 1e-3)) / 6446e9,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
                          "peak_source": "measured live: FP32 FMA-chain probe (cuopo_probe_fp32_peak); "
                                         "fields stay in shared memory, so neither HBM nor tensor cores bound it",
                          "kernel": "ssfm_kernel (fused round trips, all grid sizes)"},
