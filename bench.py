@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--sizes", type=str, default="", help="grid sizes to draw from (default 4096,8192,16384,32768); "
                     "reduced variants are for profiling only")
     ap.add_argument("--max-rt", type=int, default=MAX_RT, help="round-trip limit (default 5000)")
+    ap.add_argument("--split", action="store_true",
+                    help="N > 1: split one sweep of --count instances over the ranks (strong scaling) instead of "
+                         "giving every rank its own sweep (weak scaling, the default)")
     a = ap.parse_args()
     a.sizes = tuple(int(x) for x in a.sizes.split(",")) if a.sizes else SIZES
     return a
@@ -251,13 +254,22 @@ def run_cuopo(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    from cuopo_b200 import sweep
+    from cuopo_b200 import shard, sweep
     max_rt = args.max_rt
-    base, insts, table = sweep.random_cw_sweep(args.count, rank, n_t_choices=args.sizes, n_z=N_Z)
-    wbase, winsts, _ = sweep.random_cw_sweep(args.count, 10_000 + rank, n_t_choices=args.sizes, n_z=N_Z)
-    rec = load_rts_record(args.count) if args.sizes == SIZES and max_rt == MAX_RT else None
+    split = args.split and world > 1
+    if split:
+        # one sweep, instances dealt to the ranks by expected cost (same split on every rank)
+        base, insts, table = sweep.random_cw_sweep(args.count, 0, n_t_choices=args.sizes, n_z=N_Z)
+        mine = shard.partition(shard.instance_cost(table, N_Z), world)[rank]
+        insts = [insts[i] for i in mine]
+        table = {k: np.asarray(v)[mine] for k, v in table.items()}
+        wbase, winsts, _ = sweep.random_cw_sweep(len(insts), 10_000 + rank, n_t_choices=args.sizes, n_z=N_Z)
+    else:
+        base, insts, table = sweep.random_cw_sweep(args.count, rank, n_t_choices=args.sizes, n_z=N_Z)
+        wbase, winsts, _ = sweep.random_cw_sweep(args.count, 10_000 + rank, n_t_choices=args.sizes, n_z=N_Z)
+    rec = load_rts_record(args.count) if args.sizes == SIZES and max_rt == MAX_RT and not split else None
     cpu = None
-    if rank == 0 and args.sizes == SIZES:  # before any GPU work
+    if rank == 0 and args.sizes == SIZES and not split:  # before any GPU work
         cpu = cpu_baseline_leg(insts, rts_by_size_from(rec, table) if rec else
                                {n: MAX_RT * int(np.sum(table["n_t"] == n)) for n in SIZES})
 
@@ -286,7 +298,6 @@ def run_cuopo(args):
         w_init[off:off + x["n_t"]] = torch.from_numpy(cu.noise_host(x["n_t"], NOISE, x["seed"]))
         off += x["n_t"]
     h_out = torch.empty(total, dtype=torch.complex64).pin_memory()
-    h_res = np.zeros((3, args.count))
 
     K = max(1, args.steps)
     chunk = int(math.ceil(max_rt / K))
@@ -324,13 +335,7 @@ def run_cuopo(args):
     e2e_ms = e_start.elapsed_time(e_end)
     done = int(np.sum(flags != 0))
     conv = int(np.sum(flags == 1))
-    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
-    n = torch.tensor([done, conv], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-    dev_ms, e2e_ms = float(t[0]), float(t[1])
-    done_all, conv_all = int(n[0]), int(n[1])
+    (dev_ms, e2e_ms), (done_all, conv_all) = shard.reduce_over_ranks([dev_ms, e2e_ms], [done, conv], device=dev)
 
     # work accounting (algorithmic, this rank; all ranks solve equal-size sweeps)
     nt_o = np.array([x["n_t"] for x in insts_o])
@@ -368,16 +373,17 @@ def run_cuopo(args):
             "warmup": args.warmup,
             "ms_per_step": dev_ms / K,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong" if split else "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded parameter draws and seeded noise)",
             "config": {"workload": "batched CW sweep: 1024 instances of 2-eq MgO:PPLN (532->1064 nm, 5 mm), "
                                    "N~U[1.2,6], delta~U[-pi,pi] rad, GDD~U[-500,500] fs^2, R~U[0.90,0.99], "
                                    "grid 2^12..2^15, 100 slices/pass, tol 1e-7, max 5000 rt, noise 1e-15",
-                       "global_batch": args.count * world, "per_rank_batch": args.count,
+                       "global_batch": args.count if split else args.count * world, "per_rank_batch": len(insts),
                        "grid_sizes": list(args.sizes), "max_rt": max_rt,
-                       "round_trips_per_step": chunk, "parallelism": f"instances sharded, {world} rank(s)",
+                       "round_trips_per_step": chunk, "parallelism": (f"one sweep split over {world} ranks by expected cost" if split else
+                                       f"own sweep per rank, {world} rank(s)") + ", no collective on the data path",
                        "l2": "working set (fields of 1024 instances, 252 MB) larger than L2",
                        "solves_converged": conv_all, "solves_total": done_all,
                        "converged_decayed": int(np.sum((flags == 1) & (ps <= 1e-20))) if world == 1 else None},
@@ -392,7 +398,7 @@ def run_cuopo(args):
                          "kernel": "ssfm_kernel (fused round trips, all grid sizes)"},
             "cpu_baseline": cpu,
             "e2e": {"value": done_all / (e2e_ms * 1e-3), "unit": "solves/s",
-                    "h2d_bytes_per_step": int(total * 8 / K), "d2h_bytes_per_step": int((total * 8 + args.count * 16) / K)},
+                    "h2d_bytes_per_step": int(total * 8 / K), "d2h_bytes_per_step": int((total * 8 + len(insts) * 16) / K)},
             "gpu_launches": K * len(set(nt_o.tolist())) + 0,
             "clocks": clk,
             "validation_fp64": validation,

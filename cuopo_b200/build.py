@@ -1,6 +1,6 @@
 """Builds libcuopo_b200.so (and the drop-in CLI) in-tree with nvcc for sm_100a.
 
-Usage: python -m cuopo_b200.build [--force] [--verbose]
+Usage: python -m cuopo_b200.build [--force] [--verbose] [--cli-define NS_OPO ...] [--cli-name NAME]
 """
 from __future__ import annotations
 
@@ -27,6 +27,8 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=c11", "-Wall", "-Wextra", "-fvisibility=hidden
 
 CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu", "probe.cu"]
 C_SOURCES = ["params.c", "dat_io.c"]
+BIN = HERE / "bin"
+CLI = BIN / "cuopo"
 
 
 def _nvcc() -> str:
@@ -89,13 +91,43 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     return LIB
 
 
+def _cuda_home() -> Path:
+    return Path(_nvcc()).resolve().parent.parent
+
+
+def build_cli(defines: tuple[str, ...] = (), name: str = "cuopo", force: bool = False, verbose: bool = False) -> Path:
+    """Builds the drop-in executable (csrc/cli.cpp) against the library.
+
+    defines: the reference's compile-time switches (CW_OPO / NS_OPO,
+    THREE_EQS, PPLN / SPPLT, SIZE=, NZ=, NRT=) that set the executable's
+    defaults; run-time options override them."""
+    lib = build(force=force, verbose=verbose)
+    BIN.mkdir(exist_ok=True)
+    out = BIN / name
+    src = CSRC / "cli.cpp"
+    if not force and not _stale(out, [src, lib, INCLUDE / "cuopo.h", Path(__file__)]):
+        return out
+    cuda = _cuda_home()
+    tmp = out.with_name(out.name + ".tmp")
+    _run(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", *[f"-D{d}" for d in defines], "-I" + str(INCLUDE),
+          "-I" + str(cuda / "include"), str(src), "-o", str(tmp), "-L" + str(HERE), "-lcuopo_b200",
+          "-Wl,-rpath,$ORIGIN/..", "-L" + str(cuda / "lib64"), "-lcudart_static", "-ldl", "-lpthread", "-lrt"],
+         verbose)
+    os.replace(tmp, out)
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas", action="store_true", help="print register/spill use (-Xptxas -v)")
+    ap.add_argument("--cli-define", action="append", default=[],
+                    help="build the drop-in executable with this -D switch (repeatable, e.g. NS_OPO, THREE_EQS)")
+    ap.add_argument("--cli-name", default="cuopo", help="name of the executable under cuopo_b200/bin")
     a = ap.parse_args()
     print(build(force=a.force, verbose=a.verbose, ptxas_verbose=a.ptxas))
+    print(build_cli(tuple(a.cli_define), a.cli_name, force=a.force, verbose=a.verbose))
 
 
 if __name__ == "__main__":

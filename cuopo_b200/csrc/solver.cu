@@ -132,15 +132,20 @@ struct KernelEntry {
     {PREC, F, M, CL, IP, Ssfm<R, F, M, CL, IP>::smem_bytes(), &launch_impl<R, F, M, CL, IP, MINB>, \
      &occupancy_impl<R, F, M, CL, IP, MINB>}
 
-/* Built configurations; the first entry with M * CL == n_t is used. */
+/* Built configurations; the first entry with M * CL == n_t is used (entries
+ * are in order of measured batch throughput on the B200 where a grid size has
+ * two: 2-eq 2^13 runs faster as 2 x 4096-point CTAs, two clusters per SM, than
+ * as one 8192-point CTA; 2^15 as 8 x 4096 than as 4 x 8192).  The single-CTA
+ * entries stay reachable for callers that need one (crystal_pass_noalloc). */
 static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 1024, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 2048, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 4096, 1, false, 2),
+    CUOPO_K(float, CUOPO_F32, 2, 4096, 2, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 2, false, 1),
-    CUOPO_K(float, CUOPO_F32, 2, 8192, 4, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 4096, 8, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 8, false, 1),
     CUOPO_K(float, CUOPO_F32, 3, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 3, 1024, 1, false, 1),
@@ -166,10 +171,10 @@ static const KernelEntry k_kernels[] = {
     CUOPO_K(double, CUOPO_F64, 3, 4096, 16, true, 1),
 };
 
-static const KernelEntry *find_kernel(int precision, int F, int N)
+static const KernelEntry *find_kernel(int precision, int F, int N, bool single_cta = false)
 {
     for (const KernelEntry &k : k_kernels)
-        if (k.precision == precision && k.F == F && k.M * k.CL == N) return &k;
+        if (k.precision == precision && k.F == F && k.M * k.CL == N && (!single_cta || k.CL == 1)) return &k;
     return nullptr;
 }
 
@@ -855,8 +860,8 @@ extern "C" cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const 
                                         "(its tables live in a fixed 384 KiB device array)");
     if (p->n_z < 1 || p->n_z > CUOPO_NOALLOC_MAX_NZ)
         return cuopo_fail(CUOPO_EINVAL, "crystal_pass_noalloc: n_z must be in [1, 1024]");
-    const KernelEntry *k = find_kernel(CUOPO_F32, p->n_eqs, p->n_t);
-    if (!k || k->CL != 1) return cuopo_fail(CUOPO_EUNSUPPORTED, "crystal_pass_noalloc: no single-CTA kernel for n_t");
+    const KernelEntry *k = find_kernel(CUOPO_F32, p->n_eqs, p->n_t, true);
+    if (!k) return cuopo_fail(CUOPO_EUNSUPPORTED, "crystal_pass_noalloc: no single-CTA kernel for n_t");
     const int N = p->n_t, F = p->n_eqs, nco = (F == 2) ? 6 : 3;
 
     /* layout of the scratch array (bytes, 256-aligned pieces) */
