@@ -393,7 +393,7 @@ def run_cuopo(args):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
-                         "peak_source": "measured live: FP32 FMA-chain probe (cuopo_probe_fp32_peak); "
+                         "peak_source": "measured live: best of scalar and packed f32x2 FMA-chain probes (cuopo_probe_fp32_peak); "
                                         "fields stay in shared memory, so neither HBM nor tensor cores bound it",
                          "kernel": "ssfm_kernel (fused round trips, all grid sizes)"},
             "cpu_baseline": cpu,

@@ -47,4 +47,49 @@ template <typename C> __host__ __device__ __forceinline__ double cabs2d(C a)
     return (double)a.x * (double)a.x + (double)a.y * (double)a.y;
 }
 
+/*
+ * float2 on sm_100: the element-wise complex operations issue as one packed
+ * FP32x2 instruction (add/sub/mul/fma .f32x2) for both components instead
+ * of two scalar ones.  Each lane rounds exactly like the scalar operation
+ * (round to nearest, fused multiply-add), so the results are those of the
+ * scalar code with the same operation order; what changes is that one issue
+ * slot carries two FP32 operations, which is the limit of the SSFM kernels.
+ */
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+#define CUOPO_F32X2 1
+#define CUOPO_F2OP3(OP, A, B)                                                                                 \
+    float2 d;                                                                                                 \
+    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n " OP                  \
+        " rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"                                                             \
+        : "=f"(d.x), "=f"(d.y)                                                                                \
+        : "f"(A.x), "f"(A.y), "f"(B.x), "f"(B.y));                                                            \
+    return d;
+
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { CUOPO_F2OP3("add.rn.f32x2", a, b) }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { CUOPO_F2OP3("sub.rn.f32x2", a, b) }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { CUOPO_F2OP3("mul.rn.f32x2", a, b) }
+/* a * b + c, component-wise, fused */
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c)
+{
+    float2 d;
+    asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n mov.b64 rc, {%6, %7};\n"
+        " fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+#undef CUOPO_F2OP3
+
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return f2add(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) { return f2sub(a, b); }
+template <> __device__ __forceinline__ float2 cscale<float2, float>(float2 a, float s)
+{
+    return f2mul(a, make_float2(s, s));
+}
+template <> __device__ __forceinline__ float2 caxpy<float2, float>(float2 a, float s, float2 b)
+{
+    return f2fma(make_float2(s, s), b, a);
+}
+#endif
+
 }  // namespace cuopo

@@ -30,6 +30,34 @@ __global__ void __launch_bounds__(256) fma_probe(float *sink, int iters, float a
     if (s == 12345.678f) sink[blockIdx.x] = s;
 }
 
+/* The same with packed FP32x2 FMAs (two lanes per instruction, sm_100):
+ * the FMA pipe's throughput without any limit from instruction issue. */
+__global__ void __launch_bounds__(256) fma2_probe(float *sink, int iters, float a, float b)
+{
+    unsigned long long x[4], A, B;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(A) : "f"(a));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(B) : "f"(b));
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float u = (float)(threadIdx.x + k) * 1e-3f, v = (float)(threadIdx.x + k + 4) * 1e-3f;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(x[k]) : "f"(u), "f"(v));
+    }
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int r = 0; r < 16; r++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) asm("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[k]) : "l"(A), "l"(B));
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float u, v;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(u), "=f"(v) : "l"(x[k]));
+        s += u + v;
+    }
+    if (s == 12345.678f) sink[blockIdx.x] = s;
+}
+
 }  // namespace
 
 extern "C" cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream)
@@ -47,10 +75,13 @@ extern "C" cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream)
     cudaEventCreate(&e1);
     const int blocks = 8 * sms, threads = 256, iters = 2048;
     fma_probe<<<blocks, threads, 0, st>>>(sink, 64, 0.999f, 1e-4f); /* warm-up */
+    fma2_probe<<<blocks, threads, 0, st>>>(sink, 64, 0.999f, 1e-4f);
     double best = 0.0;
-    for (int rep = 0; rep < 3; rep++) {
+    /* the larger of scalar and packed FMA chains (8 FP32 chains per thread each) */
+    for (int rep = 0; rep < 6; rep++) {
         cudaEventRecord(e0, st);
-        fma_probe<<<blocks, threads, 0, st>>>(sink, iters, 0.999f, 1e-4f);
+        if (rep % 2 == 0) fma_probe<<<blocks, threads, 0, st>>>(sink, iters, 0.999f, 1e-4f);
+        else fma2_probe<<<blocks, threads, 0, st>>>(sink, iters, 0.999f, 1e-4f);
         cudaEventRecord(e1, st);
         cudaEventSynchronize(e1);
         float ms = 0.f;

@@ -294,8 +294,8 @@ cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const float *w_ho
                                         void *Ai, void *stream);
 
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 3
- * launches of an FMA-chain kernel over every SM); the denominator of the
- * solver's roofline.  Synchronous. */
+ * launches each of a scalar and a packed FP32x2 FMA-chain kernel over every
+ * SM); the denominator of the solver's roofline.  Synchronous. */
 cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream);
 
 /* Blocks until the plan's work on stream has finished; returns the first
