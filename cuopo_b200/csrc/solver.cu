@@ -134,9 +134,10 @@ struct KernelEntry {
 
 /* Built configurations; the first entry with M * CL == n_t is used (entries
  * are in order of measured batch throughput on the B200 where a grid size has
- * two: 2-eq 2^13 runs faster as 2 x 4096-point CTAs, two clusters per SM, than
- * as one 8192-point CTA; 2^15 as 8 x 4096 than as 4 x 8192).  The single-CTA
- * entries stay reachable for callers that need one (crystal_pass_noalloc). */
+ * two: 2-eq 2^13, 2^14 and 2^15 run faster as clusters of 2, 4 and 8
+ * 4096-point CTAs, two CTAs per SM, than as 1, 2 and 4 8192-point CTAs, one
+ * per SM).  The single-CTA entries stay reachable for callers that need one
+ * (crystal_pass_noalloc). */
 static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 1024, 1, false, 1),
@@ -144,7 +145,7 @@ static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 4096, 1, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 4096, 2, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 1, false, 1),
-    CUOPO_K(float, CUOPO_F32, 2, 8192, 2, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 4096, 4, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 4096, 8, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 8, false, 1),
     CUOPO_K(float, CUOPO_F32, 3, 512, 1, false, 1),

@@ -420,7 +420,7 @@ struct Ssfm {
         return s;
     }
 
-    static __device__ void run(const LaunchArgs &a)
+    static __device__ __forceinline__ void run(const LaunchArgs &a)
     {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         C *home = reinterpret_cast<C *>(smem_raw);
