@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--sizes", type=str, default="", help="grid sizes to draw from (default 4096,8192,16384,32768); "
                     "reduced variants are for profiling only")
     ap.add_argument("--max-rt", type=int, default=MAX_RT, help="round-trip limit (default 5000)")
+    ap.add_argument("--no-autotune", action="store_true", help="use the built-in kernel preference order")
     ap.add_argument("--split", action="store_true",
                     help="N > 1: split one sweep of --count instances over the ranks (strong scaling) instead of "
                          "giving every rank its own sweep (weak scaling, the default)")
@@ -280,6 +281,14 @@ def run_cuopo(args):
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     peak = cu.probe_fp32_peak()
+    # set-up (untimed): pick each grid size's kernel configuration by timing the candidates
+    kernels = {}
+    for n in sorted(set(int(x["n_t"]) for x in insts)):
+        if not args.no_autotune:
+            pb, _ = cu.derive_params(sweep.cw_base_inputs(n_t=n, n_z=N_Z))
+            cu.autotune(pb, cu.F32, count=max(1, sum(1 for x in insts if x["n_t"] == n)), n_rt=2)
+        m, cl = cu.kernel_config(n)
+        kernels[str(n)] = f"{cl} x {m}-point CTA" + ("s" if cl > 1 else "")
 
     # LPT order within each grid size: longest expected solves first
     order = np.argsort(-sweep.growth_estimate(table), kind="stable")
@@ -382,7 +391,9 @@ def run_cuopo(args):
                                    "grid 2^12..2^15, 100 slices/pass, tol 1e-7, max 5000 rt, noise 1e-15",
                        "global_batch": args.count if split else args.count * world, "per_rank_batch": len(insts),
                        "grid_sizes": list(args.sizes), "max_rt": max_rt,
-                       "round_trips_per_step": chunk, "parallelism": (f"one sweep split over {world} ranks by expected cost" if split else
+                       "round_trips_per_step": chunk, "kernels": kernels,
+                       "kernel_choice": "built-in order" if args.no_autotune else "autotuned (cuopo_autotune)",
+                       "parallelism": (f"one sweep split over {world} ranks by expected cost" if split else
                                        f"own sweep per rank, {world} rank(s)") + ", no collective on the data path",
                        "l2": "working set (fields of 1024 instances, 252 MB) larger than L2",
                        "solves_converged": conv_all, "solves_total": done_all,

@@ -114,6 +114,10 @@ SIGNATURES = {
     "cuopo_batch_results": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cuopo_probe_fp32_peak": (_i, [C.POINTER(_d), _vp]),
     "cuopo_crystal_pass_noalloc": (_i, [C.POINTER(Params), _vp, _vp, _vp, _vp, _vp]),
+    "cuopo_autotune": (_i, [C.POINTER(Params), _i, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_d)]),
+    "cuopo_autotune_reset": (_i, []),
+    "cuopo_kernel_select": (_i, [_i, _i, _i, _i, _i]),
+    "cuopo_kernel_config": (_i, [_i, _i, _i, C.POINTER(_i), C.POINTER(_i)]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

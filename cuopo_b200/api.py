@@ -212,6 +212,31 @@ def probe_fp32_peak(stream=None) -> float:
     return v.value
 
 
+def autotune(base: Params, precision: int = F32, count: int = 148, n_rt: int = 2) -> dict:
+    """Times every built kernel configuration for base.n_t on `count` copies of
+    the CW instance `base` (n_rt round trips each) and makes the fastest the
+    one later plans and batches of this process use (cuopo_autotune)."""
+    m, cl, ms = C.c_int(), C.c_int(), C.c_double()
+    check(load().cuopo_autotune(C.byref(base), precision, count, n_rt, C.byref(m), C.byref(cl), C.byref(ms)))
+    return {"points_per_cta": m.value, "cluster": cl.value, "ms": ms.value}
+
+
+def autotune_reset() -> None:
+    check(load().cuopo_autotune_reset())
+
+
+def kernel_select(n_t: int, points_per_cta: int, cluster: int, n_eqs: int = 2, precision: int = F32) -> None:
+    """Makes a built configuration the choice for this grid without timing."""
+    check(load().cuopo_kernel_select(precision, n_eqs, n_t, points_per_cta, cluster))
+
+
+def kernel_config(n_t: int, n_eqs: int = 2, precision: int = F32) -> tuple[int, int]:
+    """(points per CTA, CTAs per cluster) a plan for this grid would use now."""
+    m, cl = C.c_int(), C.c_int()
+    check(load().cuopo_kernel_config(precision, n_eqs, n_t, C.byref(m), C.byref(cl)))
+    return m.value, cl.value
+
+
 def sync(stream=None) -> None:
     check(load().cuopo_sync(_stream(stream) if stream is not None else None))
 

@@ -132,12 +132,13 @@ struct KernelEntry {
     {PREC, F, M, CL, IP, Ssfm<R, F, M, CL, IP>::smem_bytes(), &launch_impl<R, F, M, CL, IP, MINB>, \
      &occupancy_impl<R, F, M, CL, IP, MINB>}
 
-/* Built configurations; the first entry with M * CL == n_t is used (entries
- * are in order of measured batch throughput on the B200 where a grid size has
- * two: 2-eq 2^13, 2^14 and 2^15 run faster as clusters of 2, 4 and 8
- * 4096-point CTAs, two CTAs per SM, than as 1, 2 and 4 8192-point CTAs, one
- * per SM).  The single-CTA entries stay reachable for callers that need one
- * (crystal_pass_noalloc). */
+/* Built configurations.  Where a grid size has more than one, cuopo_autotune
+ * times them and records the winner; without a recorded choice the first
+ * entry with M * CL == n_t is used (the entries are in order of measured batch
+ * throughput on the B200: 2-eq 2^13, 2^14 and 2^15 run faster as clusters of
+ * 2, 4 and 8 4096-point CTAs, two CTAs per SM, than as 1, 2 and 4 8192-point
+ * CTAs, one per SM).  The single-CTA entries stay reachable for callers that
+ * need one (crystal_pass_noalloc). */
 static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 1024, 1, false, 1),
@@ -147,6 +148,8 @@ static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 8192, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 4096, 4, false, 2),
     CUOPO_K(float, CUOPO_F32, 2, 4096, 8, false, 2),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 2, false, 1),
+    CUOPO_K(float, CUOPO_F32, 2, 8192, 4, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 8192, 8, false, 1),
     CUOPO_K(float, CUOPO_F32, 3, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 3, 1024, 1, false, 1),
@@ -172,8 +175,25 @@ static const KernelEntry k_kernels[] = {
     CUOPO_K(double, CUOPO_F64, 3, 4096, 16, true, 1),
 };
 
+/* Autotuned choices, process-wide: (precision, F, N) -> entry. */
+struct TunedChoice {
+    int precision, F, N;
+    const KernelEntry *k;
+};
+static std::mutex g_tune_mu;
+static std::vector<TunedChoice> g_tuned;
+/* set by cuopo_autotune on its own thread while it times one candidate */
+static thread_local const KernelEntry *g_force = nullptr;
+
 static const KernelEntry *find_kernel(int precision, int F, int N, bool single_cta = false)
 {
+    if (!single_cta) {
+        if (g_force && g_force->precision == precision && g_force->F == F && g_force->M * g_force->CL == N)
+            return g_force;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (const TunedChoice &c : g_tuned)
+            if (c.precision == precision && c.F == F && c.N == N) return c.k;
+    }
     for (const KernelEntry &k : k_kernels)
         if (k.precision == precision && k.F == F && k.M * k.CL == N && (!single_cta || k.CL == 1)) return &k;
     return nullptr;
@@ -825,6 +845,114 @@ extern "C" cuopo_status cuopo_batch_results(cuopo_batch *b, double *ps, int *rts
         (e = cudaMemcpyAsync(flags, b->d_flag, sizeof(int) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "batch_results");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch_results");
+    return CUOPO_OK;
+}
+
+/* --------------------------------------------------------------- autotuner */
+
+extern "C" cuopo_status cuopo_autotune(const cuopo_params *base, int precision, int count, int n_rt, int *points_per_cta,
+                                       int *cluster, double *ms)
+{
+    if (!base || count < 1 || n_rt < 1) return cuopo_fail(CUOPO_EINVAL, "autotune: bad argument");
+    const int F = base->n_eqs, N = base->n_t;
+    std::vector<const KernelEntry *> cand;
+    for (const KernelEntry &k : k_kernels)
+        if (k.precision == precision && k.F == F && k.M * k.CL == N) cand.push_back(&k);
+    if (cand.empty()) return cuopo_fail(CUOPO_EUNSUPPORTED, "autotune: no kernel built for this (precision, n_eqs, n_t)");
+    const KernelEntry *best = cand[0];
+    double best_ms = -1.0;
+    if (cand.size() > 1) {
+        if (F != 2 || base->regime != CUOPO_CW)
+            return cuopo_fail(CUOPO_EUNSUPPORTED, "autotune: timing runs use CW 2-equation batches");
+        /* `count` copies of the base instance, seeded noise, n_rt round trips
+         * with the convergence test off (fixed work), per candidate */
+        std::vector<cuopo_instance> inst((size_t)count);
+        for (int i = 0; i < count; i++) {
+            inst[(size_t)i].n_t = N;
+            inst[(size_t)i].ap0 = base->ap0;
+            inst[(size_t)i].Rs = base->Rs;
+            inst[(size_t)i].delta = base->delta;
+            inst[(size_t)i].gdd = base->gdd;
+            inst[(size_t)i].seed = (uint64_t)i;
+        }
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaError_t e;
+        if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) {
+            if (e0) cudaEventDestroy(e0);
+            return cuda_fail(e, "autotune");
+        }
+        cuopo_status st = CUOPO_OK;
+        for (const KernelEntry *k : cand) {
+            g_force = k;
+            cuopo_batch *b = nullptr;
+            st = cuopo_batch_create(&b, base, inst.data(), count, precision);
+            if (st == CUOPO_OK) st = cuopo_batch_seed_noise(b, 1e-15, nullptr);
+            if (st == CUOPO_OK) st = cuopo_batch_run(b, 1, 0.0, 1, nullptr); /* warm-up: module load, tables */
+            if (st == CUOPO_OK) st = cuopo_batch_reset(b, nullptr);
+            float t = 0.f;
+            if (st == CUOPO_OK) {
+                cudaEventRecord(e0, nullptr);
+                st = cuopo_batch_step(b, n_rt, n_rt, 0.0, 1, nullptr);
+                cudaEventRecord(e1, nullptr);
+                if (st == CUOPO_OK && (e = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(e, "autotune");
+                if (st == CUOPO_OK) cudaEventElapsedTime(&t, e0, e1);
+            }
+            g_force = nullptr;
+            if (b) cuopo_batch_destroy(b);
+            if (st != CUOPO_OK) break;
+            if (best_ms < 0.0 || t < best_ms) {
+                best_ms = t;
+                best = k;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st != CUOPO_OK) return st;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        bool found = false;
+        for (TunedChoice &c : g_tuned)
+            if (c.precision == precision && c.F == F && c.N == N) {
+                c.k = best;
+                found = true;
+            }
+        if (!found) g_tuned.push_back(TunedChoice{precision, F, N, best});
+    }
+    if (points_per_cta) *points_per_cta = best->M;
+    if (cluster) *cluster = best->CL;
+    if (ms) *ms = best_ms;
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_kernel_select(int precision, int n_eqs, int n_t, int points_per_cta, int cluster)
+{
+    for (const KernelEntry &k : k_kernels)
+        if (k.precision == precision && k.F == n_eqs && k.M == points_per_cta && k.CL == cluster &&
+            k.M * k.CL == n_t) {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            for (TunedChoice &c : g_tuned)
+                if (c.precision == precision && c.F == n_eqs && c.N == n_t) {
+                    c.k = &k;
+                    return CUOPO_OK;
+                }
+            g_tuned.push_back(TunedChoice{precision, n_eqs, n_t, &k});
+            return CUOPO_OK;
+        }
+    return cuopo_fail(CUOPO_EUNSUPPORTED, "kernel_select: no such built configuration");
+}
+
+extern "C" cuopo_status cuopo_autotune_reset(void)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned.clear();
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_kernel_config(int precision, int n_eqs, int n_t, int *points_per_cta, int *cluster)
+{
+    const KernelEntry *k = find_kernel(precision, n_eqs, n_t);
+    if (!k) return cuopo_fail(CUOPO_EUNSUPPORTED, "kernel_config: no kernel built for this (precision, n_eqs, n_t)");
+    if (points_per_cta) *points_per_cta = k->M;
+    if (cluster) *cluster = k->CL;
     return CUOPO_OK;
 }
 

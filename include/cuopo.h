@@ -276,6 +276,27 @@ cuopo_status cuopo_batch_pending(cuopo_batch *batch, int *running, void *stream)
 cuopo_status cuopo_batch_results(cuopo_batch *batch, double *ps, int *rts, int *flags, void *stream);
 
 /*
+ * Kernel autotuner (no counterpart in the reference, which has one cuFFT plan
+ * and fixed launch shapes).  Grids that more than one built kernel
+ * configuration can run (e.g. 2^15 points as 8 CTAs of 4096 or 4 CTAs of
+ * 8192) are timed on `count` copies of the CW 2-equation instance `base`
+ * (its n_t, ap0, Rs, delta, gdd) for n_rt round trips each, and the fastest
+ * becomes the one every plan and batch created afterwards in this process
+ * uses for (precision, n_eqs, n_t).  Reports the chosen points per CTA,
+ * cluster size and its time (ms; -1 when there was one candidate).
+ * Synchronous; allocates device memory while it runs.
+ */
+cuopo_status cuopo_autotune(const cuopo_params *base, int precision, int count, int n_rt, int *points_per_cta,
+                            int *cluster, double *ms);
+/* Records a built configuration as the choice for (precision, n_eqs, n_t)
+ * without timing (CUOPO_EUNSUPPORTED if it was not built). */
+cuopo_status cuopo_kernel_select(int precision, int n_eqs, int n_t, int points_per_cta, int cluster);
+/* Forgets every autotuned or selected choice (the built-in preference order applies). */
+cuopo_status cuopo_autotune_reset(void);
+/* The configuration a plan created now would use. */
+cuopo_status cuopo_kernel_config(int precision, int n_eqs, int n_t, int *points_per_cta, int *cluster);
+
+/*
  * One crystal pass that allocates no device memory, for callers that cannot
  * call cudaMalloc: code running while a CUDA graph is being captured, or a
  * plugin in a process whose device memory belongs to another allocator.  It
