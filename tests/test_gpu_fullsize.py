@@ -1,0 +1,106 @@
+"""Full-size runs of the benchmark configurations that are not the sweep,
+FP32 fields against the FP64 solver from the same seeded inputs.  (The FP64
+GPU plans match the FP64 CPU oracle to 1e-10 at every kernel configuration,
+tests/test_gpu_ssfm.py; the CPU oracle itself would need hours here.)
+
+* single CW OPO: 2 equations, MgO:PPLN 5 mm, 532 -> 1064 nm, 4x threshold,
+  R = 0.98, 2^13 points, 100 slices, 2000 round trips from 1e-20 noise
+  (seed 0).  The signal is still in its exponential build-up at 2000
+  round trips (power ~3e-24), the regime where rounding errors are
+  amplified with the field.
+* nanosecond OPO: 3 equations, MgO:sPPLT 20 mm, 532 -> 1550 nm, 10 ns
+  Gaussian pump at 3x threshold, 2^16 points, 200 slices, 600 round trips,
+  group-velocity mismatch, dispersion and absorption on, 1e-15 noise
+  (seed 1); fields saved around the pump peak.
+
+Tolerances (measured values on the B200 in brackets): signal power per
+round trip 1e-4 [3e-5], output energy 1e-5 [8e-7].  Fields are compared
+after removing the common phase (a constant phase offset between two runs
+is physically irrelevant): the CW signal after 2000 round trips of build-up
+2e-2 [5.3e-3] -- each mode's slice factor 1 + d carries a fixed FP32
+rounding of d (relative ~1e-8 per slice for the high-frequency modes with
+|d| ~ 1), which the exponential build-up from 1e-20 noise turns into a
+per-mode amplitude error of ~1e-8 x 2e5 slices, while the power, carried
+by the low-frequency modes where |d| ~ 1e-4, stays within 3e-5.  The
+nanosecond signal and idler stay at the noise level (the 10 ns pump lasts
+~25 of the 600 round trips), so the same per-mode effect over 6e4 slices
+sets their bound: 1e-2 [2.1e-3]; the pump 1e-3.
+"""
+import numpy as np
+import pytest
+
+import cuopo_b200 as cu
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def run(p, prec, Ap, As, Ai, pump, n_rt, save_first=0, save_count=0):
+    T, w = cu.make_grids(p.n_t, p.t_rt)
+    dt = torch.complex64 if prec == cu.F32 else torch.complex128
+    d = [torch.from_numpy(x).to("cuda", dt) if x is not None else None for x in (Ap, As, Ai)]
+    dp = torch.from_numpy(pump).to("cuda", dt)
+    ps = torch.zeros(n_rt, dtype=torch.float64, device="cuda")
+    sv = [torch.zeros(p.n_t * save_count, dtype=dt, device="cuda") if save_count and x is not None else None
+          for x in (Ap, As, Ai)]
+    with cu.Plan(p, w, T, precision=prec) as plan:
+        plan.round_trips(d[0], d[1], d[2], dp, n_rt, 0, n_rt, save_p=sv[0], save_s=sv[1], save_i=sv[2],
+                         save_first=save_first, save_count=save_count, ps_hist=ps)
+        torch.cuda.synchronize()
+    h = lambda x: x.cpu().numpy().astype(np.complex128) if x is not None else None
+    return [h(x) for x in d], ps.cpu().numpy(), [h(x) for x in sv]
+
+
+def aligned_rel(a, b):
+    """Relative L2 of a against b after the best common phase."""
+    ph = np.vdot(a, b)
+    ph = ph / abs(ph) if abs(ph) > 0 else 1.0
+    return float(np.linalg.norm(a * ph - b) / np.linalg.norm(b))
+
+
+def f32(x):
+    return x.astype(np.complex64).astype(np.complex128)
+
+
+def test_single_cw_opo_2000_round_trips():
+    n_t, n_rt = 8192, 2000
+    inp = cu.default_inputs(n_t=n_t, n_z=100, n_rt=n_rt, lp_nm=532.0, lambda_um=6.970206862971646, n_thr=4.0,
+                            r_percent=98.0, lcr_mm=5.0)
+    p, _ = cu.derive_params(inp)
+    As = cu.noise_host(n_t, 1e-20, 0, 1).astype(np.complex128)
+    pump = cu.pump_cw(n_t, p.ap0).astype(np.complex128)
+    zero = np.zeros(n_t, np.complex128)
+    a = run(p, cu.F32, zero, f32(As), None, pump, n_rt)
+    b = run(p, cu.F64, zero, As, None, pump, n_rt)
+    e_ps = np.max(np.abs(a[1] - b[1]) / b[1])
+    assert b[1][-1] > 1e3 * b[1][0], "the signal must have grown"
+    assert e_ps < 1e-4, e_ps
+    e_s = aligned_rel(a[0][1], b[0][1])
+    assert e_s < 2e-2, e_s
+
+
+def test_nanosecond_three_wave_opo_600_round_trips():
+    n_t, n_rt = 65536, 600
+    inp = cu.default_inputs(crystal=cu.SPPLT, n_eqs=3, regime=cu.NS, n_t=n_t, n_z=200, n_rt=n_rt, lp_nm=532.0,
+                            ls_nm=1550.0, lambda_um=8.719670871908674, n_thr=3.0, r_percent=98.0, lcr_mm=20.0)
+    p, _ = cu.derive_params(inp)
+    As = cu.noise_host(n_t, 1e-15, 1, 1).astype(np.complex128)
+    Ai = cu.noise_host(n_t, 1e-15, 1, 2).astype(np.complex128)
+    pump = cu.pump_ns(n_t, n_rt, p.t_rt, p.ap0, inp.fwhm_ps).astype(np.complex128)
+    zero = np.zeros(n_t, np.complex128)
+    sf, sc = n_rt // 2 - 8, 16          # round trips around the pump peak
+    a = run(p, cu.F32, zero, f32(As), f32(Ai), f32(pump), n_rt, sf, sc)
+    b = run(p, cu.F64, zero, As, Ai, pump, n_rt, sf, sc)
+    e_energy = abs(a[1].sum() - b[1].sum()) / b[1].sum()
+    assert e_energy < 1e-5, e_energy
+    e_ps = np.max(np.abs(a[1] - b[1]) / b[1])
+    assert e_ps < 1e-4, e_ps
+    errs = {}
+    for f, name in enumerate(("pump", "signal", "idler")):
+        for r in (0, sc // 2, sc - 1):
+            x = a[2][f][r * n_t:(r + 1) * n_t]
+            y = b[2][f][r * n_t:(r + 1) * n_t]
+            errs[(name, sf + r)] = aligned_rel(x, y)
+    bad = {k: e for k, e in errs.items() if e > (1e-3 if k[0] == "pump" else 1e-2)}
+    assert not bad, errs
