@@ -102,6 +102,7 @@ SIGNATURES = {
     "cuopo_plan_status": (_i, [_vp, C.POINTER(_i), _i]),
     "cuopo_fft_c2c": (_i, [_vp, _vp, _i, _i, _i, _i, _vp]),
     "cuopo_batch_create": (_i, [C.POINTER(_vp), C.POINTER(Params), _vp, _i, _i]),
+    "cuopo_batch_create_inputs": (_i, [C.POINTER(_vp), _vp, _vp, _i, _i]),
     "cuopo_batch_destroy": (_i, [_vp]),
     "cuopo_batch_total_elements": (_i, [_vp, C.POINTER(C.c_long)]),
     "cuopo_batch_seed_noise": (_i, [_vp, _d, _vp]),

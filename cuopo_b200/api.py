@@ -244,18 +244,29 @@ def sync(stream=None) -> None:
 class Batch:
     """A batched CW sweep (cuopo_batch_*): many instances, one persistent launch per grid size."""
 
-    def __init__(self, base: Params, instances, precision: int = F32):
+    def __init__(self, base: Params | None, instances, precision: int = F32, seeds=None):
+        """base + instances (dicts of cuopo_instance fields), or base=None and
+        instances = a list of Inputs, one full argv-level set per instance
+        (cuopo_batch_create_inputs; seeds default to 0..count-1)."""
         from ._lib import Instance
         self._lib = load()
-        arr = (Instance * len(instances))()
-        for k, inst in enumerate(instances):
-            for name, val in inst.items():
-                setattr(arr[k], name, val)
         self.count = len(instances)
-        self.n_t = np.array([i["n_t"] for i in instances])
         self.precision = precision
         h = C.c_void_p()
-        check(self._lib.cuopo_batch_create(C.byref(h), C.byref(base), arr, len(instances), precision))
+        if base is None:
+            arr = (Inputs * self.count)(*instances)
+            sd = None
+            if seeds is not None:
+                sd = (C.c_uint64 * self.count)(*[int(x) for x in seeds])
+            self.n_t = np.array([i.n_t for i in instances])
+            check(self._lib.cuopo_batch_create_inputs(C.byref(h), arr, sd, self.count, precision))
+        else:
+            arr = (Instance * self.count)()
+            for k, inst in enumerate(instances):
+                for name, val in inst.items():
+                    setattr(arr[k], name, val)
+            self.n_t = np.array([i["n_t"] for i in instances])
+            check(self._lib.cuopo_batch_create(C.byref(h), C.byref(base), arr, self.count, precision))
         self._h = h
         n = C.c_long()
         check(self._lib.cuopo_batch_total_elements(self._h, C.byref(n)))

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <array>
 #include <mutex>
 #include <vector>
 
@@ -566,9 +567,11 @@ extern "C" cuopo_status cuopo_sync(void *stream)
 
 /* ------------------------------------------------------------------ batches */
 
+/* Instances of one launch: same number of fields, grid size, slices and
+ * modulator target; their physics tables may differ (one plan each). */
 struct BatchGroup {
-    int n_t;
-    cuopo_plan *plan;
+    int F, n_t, n_z, eom_idler;
+    std::vector<cuopo_plan *> plans; /* plans[0] supplies the launch's tables */
     std::vector<int> members;
     Instance *d_inst;
     int *d_queue;
@@ -580,13 +583,13 @@ struct BatchGroup {
 struct cuopo_batch {
     int count;
     int precision;
-    int F;
-    cuopo_params base;
-    std::vector<cuopo_instance> inst;
-    std::vector<size_t> offset;   /* element offset of each instance's signal */
+    std::vector<int> n_t, F;
+    std::vector<uint64_t> seed;
+    std::vector<size_t> offset;   /* element offset of each instance's fields */
     size_t total;                 /* total signal elements */
     void *d_pump;                 /* pump-field work buffers (n_t per instance) */
     void *d_signal;               /* signal fields, concatenated */
+    void *d_idler;                /* idler fields (same offsets) when an instance has 3 fields */
     double *d_ps;     /* per-instance resumable state (see Instance::st_*) */
     int *d_rt;
     int *d_flag;
@@ -600,7 +603,7 @@ extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
 {
     if (!b) return CUOPO_OK;
     for (BatchGroup &g : b->groups) {
-        cuopo_plan_destroy(g.plan);
+        for (cuopo_plan *pl : g.plans) cuopo_plan_destroy(pl);
         cudaFree(g.d_inst);
         cudaFree(g.d_queue);
         if (g.stream) cudaStreamDestroy(g.stream);
@@ -609,6 +612,7 @@ extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
     if (b->fork) cudaEventDestroy(b->fork);
     cudaFree(b->d_pump);
     cudaFree(b->d_signal);
+    cudaFree(b->d_idler);
     cudaFree(b->d_ps);
     cudaFree(b->d_rt);
     cudaFree(b->d_flag);
@@ -617,38 +621,54 @@ extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
     return CUOPO_OK;
 }
 
-extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params *base, const cuopo_instance *inst,
-                                           int count, int precision)
+/* Parameters that go into a plan's tables (dispersion, RK4 coefficients,
+ * grids, modulator); the rest (pump amplitude, mirrors, detuning, GDD/TOD)
+ * is per instance. */
+static std::vector<double> physics_key(const cuopo_params &p)
 {
-    if (!out || !base || !inst || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create: bad argument");
-    *out = nullptr;
-    if (base->n_eqs != 2) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW 2-equation sweeps");
-    if (base->regime != CUOPO_CW) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW sweeps");
+    return {(double)p.n_eqs, (double)p.n_t, (double)p.n_z, (double)p.regime, p.vp, p.vs, p.vi, p.b2p, p.b2s,
+            p.b2i, p.b3p, p.b3s, p.b3i, p.dk, p.kp, p.ks, p.ki, p.dz, p.alpha_crp, p.alpha_crs, p.alpha_cri,
+            (double)p.use_eom, (double)p.eom_idler, p.mod_depth, p.fpm, p.t_rt};
+}
+
+/* A batch of CW instances, each with its full parameter set. */
+static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_params> &prm,
+                                const std::vector<uint64_t> &seeds, int precision)
+{
+    const int count = (int)prm.size();
     if (precision != CUOPO_F32 && precision != CUOPO_F64)
         return cuopo_fail(CUOPO_EINVAL, "batch_create: bad precision");
+    bool any3 = false;
     for (int i = 0; i < count; i++) {
-        if (!is_pow2i(inst[i].n_t) || !find_kernel(precision, 2, inst[i].n_t))
+        const cuopo_params &p = prm[(size_t)i];
+        if (p.regime != CUOPO_CW) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW sweeps");
+        if (p.n_eqs != 2 && p.n_eqs != 3) return cuopo_fail(CUOPO_EINVAL, "batch_create: n_eqs must be 2 or 3");
+        if (!is_pow2i(p.n_t) || !find_kernel(precision, p.n_eqs, p.n_t))
             return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: an instance has an unsupported n_t");
-        if (!(inst[i].Rs >= 0.0 && inst[i].Rs <= 1.0)) return cuopo_fail(CUOPO_EINVAL, "batch_create: Rs out of [0,1]");
+        if (p.n_z < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create: n_z must be >= 1");
+        if (!(p.Rs >= 0.0 && p.Rs <= 1.0) || !(p.Ri >= 0.0 && p.Ri <= 1.0))
+            return cuopo_fail(CUOPO_EINVAL, "batch_create: reflectivity out of [0,1]");
+        any3 = any3 || p.n_eqs == 3;
     }
     cuopo_batch *b = new (std::nothrow) cuopo_batch();
     if (!b) return cuopo_fail(CUOPO_ENOMEM, "batch_create: out of host memory");
     b->count = count;
     b->precision = precision;
-    b->F = 2;
-    b->base = *base;
-    b->inst.assign(inst, inst + count);
-    b->offset.resize(count);
+    b->seed = seeds;
+    b->offset.resize((size_t)count);
     size_t off = 0;
     for (int i = 0; i < count; i++) {
-        b->offset[i] = off;
-        off += (size_t)inst[i].n_t;
+        b->n_t.push_back(prm[(size_t)i].n_t);
+        b->F.push_back(prm[(size_t)i].n_eqs);
+        b->offset[(size_t)i] = off;
+        off += (size_t)prm[(size_t)i].n_t;
     }
     b->total = off;
     const size_t esz = precision == CUOPO_F32 ? 8 : 16;
     cudaError_t e;
     if ((e = cudaMalloc(&b->d_pump, esz * off)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_signal, esz * off)) != cudaSuccess ||
+        (any3 && (e = cudaMalloc(&b->d_idler, esz * off)) != cudaSuccess) ||
         (e = cudaMalloc(&b->d_ps, sizeof(double) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rt, sizeof(int) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_flag, sizeof(int) * count)) != cudaSuccess ||
@@ -660,34 +680,54 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
     }
     cudaMemset(b->d_pump, 0, esz * off);
     cudaMemset(b->d_signal, 0, esz * off);
+    if (b->d_idler) cudaMemset(b->d_idler, 0, esz * off);
     cudaMemset(b->d_ps, 0, sizeof(double) * count);
     cudaMemset(b->d_rt, 0, sizeof(int) * count);
     cudaMemset(b->d_flag, 0, sizeof(int) * count);
     cudaMemset(b->d_calm, 0, sizeof(int) * count);
 
-    /* one plan (tables) and one persistent launch per distinct grid size */
-    std::vector<int> sizes;
-    for (int i = 0; i < count; i++)
-        if (std::find(sizes.begin(), sizes.end(), inst[i].n_t) == sizes.end()) sizes.push_back(inst[i].n_t);
-    std::sort(sizes.begin(), sizes.end(), [](int a, int c) { return a > c; });
-    b->h_inst.resize(count);
-    for (int n_t : sizes) {
-        BatchGroup g{};
-        g.n_t = n_t;
-        cuopo_params p = *base;
-        p.n_t = n_t;
-        cuopo_status st = cuopo_plan_create(&g.plan, &p, nullptr, nullptr, precision);
-        if (st != CUOPO_OK) {
-            cuopo_batch_destroy(b);
-            return st;
+    /* one persistent launch per (fields, grid size, slices, modulator target),
+     * largest grids first; one plan (tables) per distinct physics */
+    std::vector<std::array<int, 4>> keys;
+    for (const cuopo_params &p : prm) {
+        const std::array<int, 4> k = {p.n_eqs, p.n_t, p.n_z, p.eom_idler};
+        if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
+    }
+    std::sort(keys.begin(), keys.end(), [](const std::array<int, 4> &x, const std::array<int, 4> &y) {
+        return x[1] != y[1] ? x[1] > y[1] : x < y;
+    });
+    b->h_inst.resize((size_t)count);
+    for (const std::array<int, 4> &key : keys) {
+        b->groups.push_back(BatchGroup{});
+        BatchGroup &g = b->groups.back();
+        g.F = key[0];
+        g.n_t = key[1];
+        g.n_z = key[2];
+        g.eom_idler = key[3];
+        std::vector<std::vector<double>> pkeys;
+        std::vector<int> plan_of;
+        for (int i = 0; i < count; i++) {
+            const cuopo_params &p = prm[(size_t)i];
+            if (p.n_eqs != g.F || p.n_t != g.n_t || p.n_z != g.n_z || p.eom_idler != g.eom_idler) continue;
+            g.members.push_back(i);
+            const std::vector<double> pk = physics_key(p);
+            size_t q = std::find(pkeys.begin(), pkeys.end(), pk) - pkeys.begin();
+            if (q == pkeys.size()) {
+                cuopo_plan *pl = nullptr;
+                cuopo_status st = cuopo_plan_create(&pl, &p, nullptr, nullptr, precision);
+                if (st != CUOPO_OK) {
+                    cuopo_batch_destroy(b);
+                    return st;
+                }
+                g.plans.push_back(pl);
+                pkeys.push_back(pk);
+            }
+            plan_of.push_back((int)q);
         }
-        for (int i = 0; i < count; i++)
-            if (inst[i].n_t == n_t) g.members.push_back(i);
-        const KernelEntry *k = find_kernel(precision, 2, n_t);
+        const KernelEntry *k = find_kernel(precision, g.F, g.n_t);
         /* persistent grid: as many clusters as can be resident at once */
         const int occ = k->occ();
         if (occ < 1) {
-            b->groups.push_back(g);
             cuopo_batch_destroy(b);
             return cuopo_fail(CUOPO_ECUDA, "batch_create: kernel does not fit on the device");
         }
@@ -696,40 +736,75 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
             (e = cudaMalloc(&g.d_queue, sizeof(int))) != cudaSuccess ||
             (e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming)) != cudaSuccess) {
-            b->groups.push_back(g);
             cuopo_batch_destroy(b);
             return cuda_fail(e, "batch_create");
         }
         std::vector<Instance> hi(g.members.size());
         for (size_t j = 0; j < g.members.size(); j++) {
             const int i = g.members[j];
+            const cuopo_params &p = prm[(size_t)i];
+            const cuopo_plan *pl = g.plans[(size_t)plan_of[j]];
             Instance &I = hi[j];
             std::memset(&I, 0, sizeof(I));
-            I.Ap = (char *)b->d_pump + esz * b->offset[i];
-            I.As = (char *)b->d_signal + esz * b->offset[i];
-            I.Ai = nullptr;
+            I.Ap = (char *)b->d_pump + esz * b->offset[(size_t)i];
+            I.As = (char *)b->d_signal + esz * b->offset[(size_t)i];
+            I.Ai = g.F == 3 ? (char *)b->d_idler + esz * b->offset[(size_t)i] : nullptr;
             I.pump = nullptr;
-            I.ap0 = inst[i].ap0;
-            cuopo_params pi = p;
-            pi.Rs = inst[i].Rs;
-            pi.delta = inst[i].delta;
-            pi.gdd = inst[i].gdd;
-            cavity_factors(pi, I);
+            I.ap0 = p.ap0;
+            cavity_factors(p, I);
+            I.disp = pl->d_disp;
+            I.rk = pl->d_rk;
+            I.w = pl->d_w;
+            I.eom = (p.use_eom && pl->d_eom) ? pl->d_eom : nullptr;
+            I.h6 = pl->h6;
             I.st_ps = b->d_ps + i;
             I.st_rt = b->d_rt + i;
             I.st_flag = b->d_flag + i;
             I.st_calm = b->d_calm + i;
-            b->h_inst[i] = I;
+            b->h_inst[(size_t)i] = I;
         }
         if ((e = cudaMemcpy(g.d_inst, hi.data(), sizeof(Instance) * hi.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
-            b->groups.push_back(g);
             cuopo_batch_destroy(b);
             return cuda_fail(e, "batch_create: upload");
         }
-        b->groups.push_back(g);
     }
     *out = b;
     return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params *base, const cuopo_instance *inst,
+                                           int count, int precision)
+{
+    if (!out || !base || !inst || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create: bad argument");
+    *out = nullptr;
+    std::vector<cuopo_params> prm((size_t)count, *base);
+    std::vector<uint64_t> seeds((size_t)count);
+    for (int i = 0; i < count; i++) {
+        cuopo_params &p = prm[(size_t)i];
+        p.n_t = inst[i].n_t;
+        p.ap0 = inst[i].ap0;
+        p.Rs = inst[i].Rs;
+        p.delta = inst[i].delta;
+        p.gdd = inst[i].gdd;
+        seeds[(size_t)i] = inst[i].seed;
+    }
+    return batch_build(out, prm, seeds, precision);
+}
+
+extern "C" cuopo_status cuopo_batch_create_inputs(cuopo_batch **out, const cuopo_inputs *in, const uint64_t *seeds,
+                                                  int count, int precision)
+{
+    if (!out || !in || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create_inputs: bad argument");
+    *out = nullptr;
+    std::vector<cuopo_params> prm((size_t)count);
+    std::vector<uint64_t> sd((size_t)count);
+    for (int i = 0; i < count; i++) {
+        cuopo_info info;
+        cuopo_status st = cuopo_derive_params(&in[i], &prm[(size_t)i], &info);
+        if (st != CUOPO_OK) return st;
+        sd[(size_t)i] = seeds ? seeds[i] : (uint64_t)i;
+    }
+    return batch_build(out, prm, sd, precision);
 }
 
 extern "C" cuopo_status cuopo_batch_total_elements(const cuopo_batch *b, long *n)
@@ -744,8 +819,11 @@ extern "C" cuopo_status cuopo_batch_seed_noise(cuopo_batch *b, double sigma, voi
     if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_seed_noise: NULL batch");
     if (b->precision != CUOPO_F32) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_seed_noise: F32 batches only");
     for (int i = 0; i < b->count; i++) {
-        cuopo_status st = cuopo_noise_device((char *)b->d_signal + 8 * b->offset[i], b->inst[i].n_t, sigma,
-                                             b->inst[i].seed, 0, stream);
+        cuopo_status st = cuopo_noise_device((char *)b->d_signal + 8 * b->offset[(size_t)i], b->n_t[(size_t)i], sigma,
+                                             b->seed[(size_t)i], 0, stream);
+        if (st == CUOPO_OK && b->F[(size_t)i] == 3)
+            st = cuopo_noise_device((char *)b->d_idler + 8 * b->offset[(size_t)i], b->n_t[(size_t)i], sigma,
+                                    b->seed[(size_t)i], 1, stream);
         if (st != CUOPO_OK) return st;
     }
     return CUOPO_OK;
@@ -795,7 +873,7 @@ extern "C" cuopo_status cuopo_batch_step(cuopo_batch *b, int chunk, int max_rt, 
         if ((e = cudaStreamWaitEvent(g.stream, b->fork, 0)) != cudaSuccess) return cuda_fail(e, "batch_step");
         if ((e = cudaMemsetAsync(g.d_queue, 0, sizeof(int), g.stream)) != cudaSuccess)
             return cuda_fail(e, "batch_step");
-        LaunchArgs a = base_args(g.plan);
+        LaunchArgs a = base_args(g.plans[0]);
         a.inst = g.d_inst;
         a.n_inst = (int)g.members.size();
         a.queue = g.d_queue;
@@ -803,7 +881,7 @@ extern "C" cuopo_status cuopo_batch_step(cuopo_batch *b, int chunk, int max_rt, 
         a.max_rt = max_rt;
         a.tol = tol;
         a.patience = patience;
-        cuopo_status s2 = launch(g.plan, a, g.grid, g.stream);
+        cuopo_status s2 = launch(g.plans[0], a, g.grid, g.stream);
         if (s2 != CUOPO_OK) return s2;
         if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess) return cuda_fail(e, "batch_step");
         if ((e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess) return cuda_fail(e, "batch_step");

@@ -83,6 +83,11 @@ struct Instance {
     double *st_ps;
     int *st_calm;
     int *st_flag;
+    /* the instance's own physics tables (batches whose instances differ in
+     * crystal, wavelengths, length or modulator); NULL disp: the launch's */
+    const void *disp, *rk, *eom;
+    const float *w;
+    double h6;
 };
 
 struct LaunchArgs {
@@ -437,11 +442,6 @@ struct Ssfm {
         StageTwiddles<M, C> tw;
         tw.init(t, twtab);
         __syncthreads();
-        const Tables &tab = a.tab;
-        const R h6 = (R)tab.h6;
-        const C *__restrict__ rk = reinterpret_cast<const C *>(tab.rk);
-        const C *__restrict__ disp = reinterpret_cast<const C *>(tab.disp);
-        const float *__restrict__ wtab = tab.w + (size_t)rank * M;
 
         bool first = true;
         for (;;) {
@@ -458,6 +458,21 @@ struct Ssfm {
             }
             first = false;
             const Instance &I = a.inst ? a.inst[idx] : a.single;
+            /* this instance's tables: its own where it has them, else the launch's */
+            Tables tab = a.tab;
+            int use_eom = a.use_eom;
+            if (I.disp) {
+                tab.disp = I.disp;
+                tab.rk = I.rk;
+                tab.w = I.w;
+                tab.h6 = I.h6;
+                tab.eom = I.eom;
+                use_eom = I.eom != nullptr;
+            }
+            const R h6 = (R)tab.h6;
+            const C *__restrict__ rk = reinterpret_cast<const C *>(tab.rk);
+            const C *__restrict__ disp = reinterpret_cast<const C *>(tab.disp);
+            const float *__restrict__ wtab = tab.w + (size_t)rank * M;
             int rt_begin = I.rt_begin, rt_count = I.rt_count, patience = I.patience, calm = 0;
             double tol = I.tol, prev_ps = -1.0;
             if (I.st_flag) {
@@ -536,7 +551,7 @@ struct Ssfm {
                      * signal and idler go to the frequency domain, the pump stays in time */
                     Ops op{};
                     op.rk0 = last_row;
-                    op.eom = a.use_eom;
+                    op.eom = use_eom;
                     const unsigned res = ALL & ~1u;
                     cross(home, ALL, res, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
@@ -549,7 +564,7 @@ struct Ssfm {
                     cross(home, res, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 } else {
                     end.rk0 = last_row;
-                    end.eom = a.use_eom;
+                    end.eom = use_eom;
                     frame_back(end, th);
                     cross(home, ALL, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 }

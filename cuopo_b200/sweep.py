@@ -51,3 +51,24 @@ def growth_estimate(table, noise_sigma: float = 1e-15) -> np.ndarray:
     used only to order work (longest first)."""
     g = 2.0 * (np.sqrt(table["n_thr"]) - 1.0) * (1.0 - table["refl"])
     return np.log(0.2 / (2 * noise_sigma ** 2)) / np.maximum(g, 1e-6)
+
+
+def script_sweep(base: "api.Inputs | None" = None, **axes) -> list:
+    """The nested loops of the reference's sweep script (src/cuOPO.sh:91-174)
+    as a list of per-instance inputs: the Cartesian product of the given
+    axes over any cuopo_inputs fields (lp_nm, lambda_um, n_thr, r_percent,
+    delta, gdd_percent, tod_percent, use_eom, mod_depth_pi, freq_det_mhz,
+    lcr_mm, n_t, n_z, n_eqs, ...), the first axis outermost.  Run them with
+    api.Batch(None, inputs)."""
+    import ctypes
+    import itertools
+    base = base if base is not None else cw_base_inputs()
+    names = list(axes)
+    out = []
+    for vals in itertools.product(*(axes[n] for n in names)):
+        inp = api.Inputs()
+        ctypes.pointer(inp)[0] = base
+        for n, v in zip(names, vals):
+            setattr(inp, n, v)
+        out.append(inp)
+    return out

@@ -244,14 +244,25 @@ typedef struct {
 
 typedef struct cuopo_batch cuopo_batch;
 
-/* base supplies the crystal and everything not in cuopo_instance. */
+/* base supplies the crystal and everything not in cuopo_instance (CW,
+ * 2 or 3 equations). */
 cuopo_status cuopo_batch_create(cuopo_batch **batch, const cuopo_params *base,
                                 const cuopo_instance *inst, int count, int precision);
+/* A sweep of points of the reference's shell script (src/cuOPO.sh:91-174):
+ * every instance has its own argv-level inputs -- pump wavelength, grating
+ * period, crystal length, pump ratio, reflectivity, detuning, GDD and TOD
+ * compensation, modulator, grid size, slices, 2 or 3 equations (CW) --
+ * derived as cuopo_derive_params does.  Instances with equal physics share
+ * one set of tables; all instances of a grid size run in one persistent
+ * launch.  seeds: per-instance noise seeds, or NULL for 0..count-1. */
+cuopo_status cuopo_batch_create_inputs(cuopo_batch **batch, const cuopo_inputs *in, const uint64_t *seeds,
+                                       int count, int precision);
 cuopo_status cuopo_batch_destroy(cuopo_batch *batch);
 /* Number of signal values of all instances (sum of n_t). */
 cuopo_status cuopo_batch_total_elements(const cuopo_batch *batch, long *n);
 /* Signal of every instance := seeded noise (cuopo_noise_device with the
- * instance's seed, stream id 0). */
+ * instance's seed, stream id 0); idler of 3-equation instances likewise
+ * with stream id 1. */
 cuopo_status cuopo_batch_seed_noise(cuopo_batch *batch, double sigma, void *stream);
 /* Copies all signals in/out: instances concatenated in creation order. */
 cuopo_status cuopo_batch_set_signal(cuopo_batch *batch, const void *src, int src_on_device, void *stream);
