@@ -86,6 +86,15 @@ def flops_per_instance_rt(n_t: int, gdd: float) -> float:
     return N_Z * per_slice + cav
 
 
+def measured_hbm_gbs() -> float:
+    """HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else
+    the earlier measurement on the same pool (6650 GB/s)."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
 
@@ -400,7 +409,7 @@ def run_cuopo(args):
                        "converged_decayed": int(np.sum((flags == 1) & (ps <= 1e-20))) if world == 1 else None},
             "slices_per_s": slices * world / (dev_ms * 1e-3),
             "point_slices_per_s": pt_slices * world / (dev_ms * 1e-3),
-            "hbm_frac": (hbm_bytes / (dev_ms * 1e-3)) / 6446e9,
+            "hbm_frac": (hbm_bytes / (dev_ms * 1e-3)) / (measured_hbm_gbs() * 1e9),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
