@@ -305,6 +305,12 @@ class Batch:
         else:
             check(self._lib.cuopo_batch_get_signal(self._h, dst.data_ptr(), int(dst.is_cuda), _stream(stream)))
 
+    def history(self, i: int, n: int, stream=None) -> np.ndarray:
+        """Signal power per round trip of nanosecond instance i (first n values)."""
+        out = np.zeros(n)
+        check(self._lib.cuopo_batch_history(self._h, i, out.ctypes.data, n, _stream(stream)))
+        return out
+
     def run(self, max_rt: int, tol: float, patience: int = 1, stream=None) -> None:
         """Solve every instance from round trip 0 (one persistent launch per grid size)."""
         check(self._lib.cuopo_batch_run(self._h, max_rt, tol, patience, _stream(stream)))

@@ -570,7 +570,7 @@ extern "C" cuopo_status cuopo_sync(void *stream)
 /* Instances of one launch: same number of fields, grid size, slices and
  * modulator target; their physics tables may differ (one plan each). */
 struct BatchGroup {
-    int F, n_t, n_z, eom_idler;
+    int F, n_t, n_z, eom_idler, regime;
     std::vector<cuopo_plan *> plans; /* plans[0] supplies the launch's tables */
     std::vector<int> members;
     Instance *d_inst;
@@ -590,6 +590,10 @@ struct cuopo_batch {
     void *d_pump;                 /* pump-field work buffers (n_t per instance) */
     void *d_signal;               /* signal fields, concatenated */
     void *d_idler;                /* idler fields (same offsets) when an instance has 3 fields */
+    void *d_win;                  /* nanosecond instances: their pump windows (n_t x n_rt each) */
+    double *d_hist;               /* nanosecond instances: signal power per round trip */
+    std::vector<long> hist_off;   /* offset into d_hist, -1 for CW instances */
+    std::vector<int> n_rt;        /* pump-window round trips (nanosecond instances) */
     double *d_ps;     /* per-instance resumable state (see Instance::st_*) */
     int *d_rt;
     int *d_flag;
@@ -613,6 +617,8 @@ extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
     cudaFree(b->d_pump);
     cudaFree(b->d_signal);
     cudaFree(b->d_idler);
+    cudaFree(b->d_win);
+    cudaFree(b->d_hist);
     cudaFree(b->d_ps);
     cudaFree(b->d_rt);
     cudaFree(b->d_flag);
@@ -631,17 +637,31 @@ static std::vector<double> physics_key(const cuopo_params &p)
             (double)p.use_eom, (double)p.eom_idler, p.mod_depth, p.fpm, p.t_rt};
 }
 
-/* A batch of CW instances, each with its full parameter set. */
+/* A batch of instances, each with its full parameter set; nanosecond
+ * instances also with their pump window's round trips and pulse width
+ * (ns_rt / ns_fwhm, NULL when there are none). */
 static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_params> &prm,
-                                const std::vector<uint64_t> &seeds, int precision)
+                                const std::vector<uint64_t> &seeds, int precision,
+                                const std::vector<int> *ns_rt = nullptr,
+                                const std::vector<double> *ns_fwhm = nullptr)
 {
     const int count = (int)prm.size();
     if (precision != CUOPO_F32 && precision != CUOPO_F64)
         return cuopo_fail(CUOPO_EINVAL, "batch_create: bad precision");
     bool any3 = false;
+    size_t win_total = 0, hist_total = 0;
     for (int i = 0; i < count; i++) {
         const cuopo_params &p = prm[(size_t)i];
-        if (p.regime != CUOPO_CW) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: batches are CW sweeps");
+        if (p.regime == CUOPO_NS) {
+            if (!ns_rt || !ns_fwhm)
+                return cuopo_fail(CUOPO_EUNSUPPORTED,
+                                  "batch_create: nanosecond instances need cuopo_batch_create_inputs (n_rt, pulse)");
+            if ((*ns_rt)[(size_t)i] < 2) return cuopo_fail(CUOPO_EINVAL, "batch_create: nanosecond n_rt must be >= 2");
+            win_total += (size_t)p.n_t * (size_t)(*ns_rt)[(size_t)i];
+            hist_total += (size_t)(*ns_rt)[(size_t)i];
+        } else if (p.regime != CUOPO_CW) {
+            return cuopo_fail(CUOPO_EINVAL, "batch_create: bad regime");
+        }
         if (p.n_eqs != 2 && p.n_eqs != 3) return cuopo_fail(CUOPO_EINVAL, "batch_create: n_eqs must be 2 or 3");
         if (!is_pow2i(p.n_t) || !find_kernel(precision, p.n_eqs, p.n_t))
             return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_create: an instance has an unsupported n_t");
@@ -669,6 +689,8 @@ static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_param
     if ((e = cudaMalloc(&b->d_pump, esz * off)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_signal, esz * off)) != cudaSuccess ||
         (any3 && (e = cudaMalloc(&b->d_idler, esz * off)) != cudaSuccess) ||
+        (win_total && (e = cudaMalloc(&b->d_win, esz * win_total)) != cudaSuccess) ||
+        (hist_total && (e = cudaMalloc(&b->d_hist, sizeof(double) * hist_total)) != cudaSuccess) ||
         (e = cudaMalloc(&b->d_ps, sizeof(double) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rt, sizeof(int) * count)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_flag, sizeof(int) * count)) != cudaSuccess ||
@@ -685,30 +707,70 @@ static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_param
     cudaMemset(b->d_rt, 0, sizeof(int) * count);
     cudaMemset(b->d_flag, 0, sizeof(int) * count);
     cudaMemset(b->d_calm, 0, sizeof(int) * count);
+    if (b->d_hist) cudaMemset(b->d_hist, 0, sizeof(double) * hist_total);
+    /* nanosecond pump windows (cuOPO.cu:164-175,243-248), built on the host as
+     * the reference does, one per nanosecond instance */
+    std::vector<size_t> win_off((size_t)count, 0);
+    b->hist_off.assign((size_t)count, -1);
+    b->n_rt.assign((size_t)count, 0);
+    {
+        size_t wo = 0, ho = 0;
+        std::vector<float> wf;
+        std::vector<double> wd;
+        for (int i = 0; i < count; i++) {
+            const cuopo_params &p = prm[(size_t)i];
+            if (p.regime != CUOPO_NS) continue;
+            const int nrt = (*ns_rt)[(size_t)i];
+            const size_t n = (size_t)p.n_t * (size_t)nrt;
+            wf.resize(2 * n);
+            cuopo_status st = cuopo_pump_ns(wf.data(), p.n_t, nrt, p.t_rt, p.ap0, (*ns_fwhm)[(size_t)i]);
+            if (st != CUOPO_OK) {
+                cuopo_batch_destroy(b);
+                return st;
+            }
+            const void *src = wf.data();
+            if (precision == CUOPO_F64) {
+                wd.assign(wf.begin(), wf.end());
+                src = wd.data();
+            }
+            if ((e = cudaMemcpy((char *)b->d_win + esz * wo, src, esz * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
+                cuopo_batch_destroy(b);
+                return cuda_fail(e, "batch_create: pump windows");
+            }
+            win_off[(size_t)i] = wo;
+            b->hist_off[(size_t)i] = (long)ho;
+            b->n_rt[(size_t)i] = nrt;
+            wo += n;
+            ho += (size_t)nrt;
+        }
+    }
 
-    /* one persistent launch per (fields, grid size, slices, modulator target),
+    /* one persistent launch per (fields, grid size, slices, modulator target, regime),
      * largest grids first; one plan (tables) per distinct physics */
-    std::vector<std::array<int, 4>> keys;
+    std::vector<std::array<int, 5>> keys;
     for (const cuopo_params &p : prm) {
-        const std::array<int, 4> k = {p.n_eqs, p.n_t, p.n_z, p.eom_idler};
+        const std::array<int, 5> k = {p.n_eqs, p.n_t, p.n_z, p.eom_idler, p.regime};
         if (std::find(keys.begin(), keys.end(), k) == keys.end()) keys.push_back(k);
     }
-    std::sort(keys.begin(), keys.end(), [](const std::array<int, 4> &x, const std::array<int, 4> &y) {
+    std::sort(keys.begin(), keys.end(), [](const std::array<int, 5> &x, const std::array<int, 5> &y) {
         return x[1] != y[1] ? x[1] > y[1] : x < y;
     });
     b->h_inst.resize((size_t)count);
-    for (const std::array<int, 4> &key : keys) {
+    for (const std::array<int, 5> &key : keys) {
         b->groups.push_back(BatchGroup{});
         BatchGroup &g = b->groups.back();
         g.F = key[0];
         g.n_t = key[1];
         g.n_z = key[2];
         g.eom_idler = key[3];
+        g.regime = key[4];
         std::vector<std::vector<double>> pkeys;
         std::vector<int> plan_of;
         for (int i = 0; i < count; i++) {
             const cuopo_params &p = prm[(size_t)i];
-            if (p.n_eqs != g.F || p.n_t != g.n_t || p.n_z != g.n_z || p.eom_idler != g.eom_idler) continue;
+            if (p.n_eqs != g.F || p.n_t != g.n_t || p.n_z != g.n_z || p.eom_idler != g.eom_idler ||
+                p.regime != g.regime)
+                continue;
             g.members.push_back(i);
             const std::vector<double> pk = physics_key(p);
             size_t q = std::find(pkeys.begin(), pkeys.end(), pk) - pkeys.begin();
@@ -751,6 +813,11 @@ static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_param
             I.Ai = g.F == 3 ? (char *)b->d_idler + esz * b->offset[(size_t)i] : nullptr;
             I.pump = nullptr;
             I.ap0 = p.ap0;
+            if (p.regime == CUOPO_NS) {
+                I.pump = (char *)b->d_win + esz * win_off[(size_t)i];
+                I.n_rt_total = b->n_rt[(size_t)i];
+                I.ps_hist = b->d_hist + b->hist_off[(size_t)i];
+            }
             cavity_factors(p, I);
             I.disp = pl->d_disp;
             I.rk = pl->d_rk;
@@ -798,13 +865,17 @@ extern "C" cuopo_status cuopo_batch_create_inputs(cuopo_batch **out, const cuopo
     *out = nullptr;
     std::vector<cuopo_params> prm((size_t)count);
     std::vector<uint64_t> sd((size_t)count);
+    std::vector<int> nrt((size_t)count);
+    std::vector<double> fwhm((size_t)count);
     for (int i = 0; i < count; i++) {
         cuopo_info info;
         cuopo_status st = cuopo_derive_params(&in[i], &prm[(size_t)i], &info);
         if (st != CUOPO_OK) return st;
         sd[(size_t)i] = seeds ? seeds[i] : (uint64_t)i;
+        nrt[(size_t)i] = in[i].n_rt;
+        fwhm[(size_t)i] = in[i].fwhm_ps;
     }
-    return batch_build(out, prm, sd, precision);
+    return batch_build(out, prm, sd, precision, &nrt, &fwhm);
 }
 
 extern "C" cuopo_status cuopo_batch_total_elements(const cuopo_batch *b, long *n)
@@ -859,6 +930,12 @@ extern "C" cuopo_status cuopo_batch_reset(cuopo_batch *b, void *stream)
         (e = cudaMemsetAsync(b->d_calm, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(b->d_ps, 0, sizeof(double) * b->count, st)) != cudaSuccess)
         return cuda_fail(e, "batch_reset");
+    if (b->d_hist) {
+        size_t n = 0;
+        for (int v : b->n_rt) n += (size_t)v;
+        if ((e = cudaMemsetAsync(b->d_hist, 0, sizeof(double) * n, st)) != cudaSuccess)
+            return cuda_fail(e, "batch_reset");
+    }
     return CUOPO_OK;
 }
 
@@ -924,6 +1001,19 @@ extern "C" cuopo_status cuopo_batch_results(cuopo_batch *b, double *ps, int *rts
         return cuda_fail(e, "batch_results");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch_results");
     return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_history(cuopo_batch *b, int i, double *ps, int n, void *stream)
+{
+    if (!b || !ps || i < 0 || i >= b->count) return cuopo_fail(CUOPO_EINVAL, "batch_history: bad argument");
+    if (b->hist_off[(size_t)i] < 0)
+        return cuopo_fail(CUOPO_EINVAL, "batch_history: only nanosecond instances keep a history");
+    const int m = std::min(n, b->n_rt[(size_t)i]);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(ps, b->d_hist + b->hist_off[(size_t)i], sizeof(double) * (size_t)m,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? CUOPO_OK : cuda_fail(e, "batch_history");
 }
 
 /* --------------------------------------------------------------- autotuner */

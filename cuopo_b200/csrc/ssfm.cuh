@@ -242,6 +242,13 @@ struct Ssfm {
         }
     }
 
+    /* Round-trip limit of a batch instance: the launch's, and for a
+     * nanosecond instance also the end of its pump window. */
+    static __device__ __forceinline__ int rt_limit(const LaunchArgs &a, const Instance &I)
+    {
+        return (a.regime == 1 && I.n_rt_total > 0) ? min(a.max_rt, I.n_rt_total) : a.max_rt;
+    }
+
     static __device__ __forceinline__ void xsync()
     {
         if constexpr (CL > 1) cg::this_cluster().sync();
@@ -479,7 +486,7 @@ struct Ssfm {
                 /* batch instance: resume from its saved state, skip if done */
                 if (*(volatile int *)I.st_flag != 0) continue;
                 rt_begin = *(volatile int *)I.st_rt;
-                rt_count = min(a.chunk, a.max_rt - rt_begin);
+                rt_count = min(a.chunk, rt_limit(a, I) - rt_begin);
                 prev_ps = rt_begin > 0 ? *(volatile double *)I.st_ps : -1.0;
                 calm = *(volatile int *)I.st_calm;
                 tol = a.tol;
@@ -578,7 +585,8 @@ struct Ssfm {
                     for (int c = 0; c < CL; c++) part += *peer(&red_cl, c);
                 }
                 ps = part * tab.inv_n;
-                if (rank == 0 && t == 0 && I.ps_hist) I.ps_hist[rt - rt_begin] = ps;
+                /* single launches record from rt_begin, batch instances by round trip */
+                if (rank == 0 && t == 0 && I.ps_hist) I.ps_hist[I.st_flag ? rt : rt - rt_begin] = ps;
                 if (!(ps == ps) || ps > 1.0e300) {
                     if (rank == 0 && t == 0 && a.status) atomicCAS(a.status, 0, (int)ST_NONFINITE);
                     flag = ST_NONFINITE;
@@ -609,7 +617,7 @@ struct Ssfm {
                     *I.st_rt = rt_begin + rts;
                     *I.st_ps = ps;
                     *I.st_calm = calm;
-                    *I.st_flag = flag != 0 ? flag : (rt_begin + rts >= a.max_rt ? (int)ST_LIMIT : 0);
+                    *I.st_flag = flag != 0 ? flag : (rt_begin + rts >= rt_limit(a, I) ? (int)ST_LIMIT : 0);
                 }
             }
             bar();

@@ -251,12 +251,18 @@ cuopo_status cuopo_batch_create(cuopo_batch **batch, const cuopo_params *base,
 /* A sweep of points of the reference's shell script (src/cuOPO.sh:91-174):
  * every instance has its own argv-level inputs -- pump wavelength, grating
  * period, crystal length, pump ratio, reflectivity, detuning, GDD and TOD
- * compensation, modulator, grid size, slices, 2 or 3 equations (CW) --
- * derived as cuopo_derive_params does.  Instances with equal physics share
- * one set of tables; all instances of a grid size run in one persistent
- * launch.  seeds: per-instance noise seeds, or NULL for 0..count-1. */
+ * compensation, modulator, grid size, slices, 2 or 3 equations, CW or
+ * nanosecond regime -- derived as cuopo_derive_params does.  A nanosecond
+ * instance gets its own Gaussian pump window of n_t * n_rt points
+ * (cuOPO.cu:164-175,243-248) and runs at most its n_rt round trips.
+ * Instances with equal physics share one set of tables; all instances of a
+ * grid size run in one persistent launch.  seeds: per-instance noise
+ * seeds, or NULL for 0..count-1. */
 cuopo_status cuopo_batch_create_inputs(cuopo_batch **batch, const cuopo_inputs *in, const uint64_t *seeds,
                                        int count, int precision);
+/* Signal power (1/n_t) sum |As|^2 after each round trip of nanosecond
+ * instance i (its n_rt values; the first n are copied).  Synchronous. */
+cuopo_status cuopo_batch_history(cuopo_batch *batch, int i, double *ps, int n, void *stream);
 cuopo_status cuopo_batch_destroy(cuopo_batch *batch);
 /* Number of signal values of all instances (sum of n_t). */
 cuopo_status cuopo_batch_total_elements(const cuopo_batch *batch, long *n);

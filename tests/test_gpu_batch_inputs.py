@@ -1,7 +1,7 @@
 """Sweeps of the reference's shell script as one batch
 (cuopo_batch_create_inputs): every instance with its own argv-level inputs,
-2 and 3 equations, different crystals, lengths, grating periods,
-modulator settings and grid sizes in one batch.
+2 and 3 equations, CW and nanosecond regimes, different crystals, lengths,
+grating periods, modulator settings and grid sizes in one batch.
 
 Each instance is checked against the single-instance entry point started
 from the same noise: bit-identical signal and signal power (same kernel
@@ -92,8 +92,45 @@ def test_fp64_batch_of_inputs_vs_oracle():
         assert rel_l2(got[k], A[1]) < 1e-10, k
 
 
-def test_mixed_batch_rejects_ns_and_bad_sizes():
-    bad = [cu.default_inputs(regime=cu.NS, n_t=1024, n_z=2)]
-    with pytest.raises(cu.CuopoError) as e:
-        cu.Batch(None, bad)
+def test_nanosecond_batch_matches_single_instance_calls():
+    """Nanosecond 3-wave instances with different pump ratios, pulse widths,
+    crystal lengths and pump windows: each runs its own window (ReadPump
+    offsets included) for its n_rt round trips; fields and the power per
+    round trip equal single-instance runs bit for bit."""
+    base = cu.default_inputs(crystal=cu.SPPLT, n_eqs=3, regime=cu.NS, n_t=1024, n_z=4, lp_nm=532.0, ls_nm=1550.0,
+                             lambda_um=8.719670871908674, r_percent=97.0)
+    ins = sweep.script_sweep(base, n_thr=[2.0, 3.0], lcr_mm=[10.0, 20.0], n_rt=[5, 8])
+    for k, x in enumerate(ins):
+        x.fwhm_ps = 2000.0 + 500.0 * k
+    seeds = np.arange(len(ins)) + 7
+    with cu.Batch(None, ins, seeds=seeds) as b:
+        b.seed_noise(SIGMA)
+        b.run(50, 0.0)           # each instance stops at its own n_rt
+        ps, rts, flags = b.results()
+        got = signals(b)
+        hist = [b.history(k, ins[k].n_rt) for k in range(len(ins))]
+    assert [int(r) for r in rts] == [x.n_rt for x in ins]
+    for k, inp in enumerate(ins):
+        p, _ = cu.derive_params(inp)
+        pump = cu.pump_ns(p.n_t, inp.n_rt, p.t_rt, p.ap0, inp.fwhm_ps)
+        with cu.Plan(p) as plan:
+            Ap = torch.zeros(p.n_t, dtype=torch.complex64, device="cuda")
+            As = torch.from_numpy(cu.noise_host(p.n_t, SIGMA, int(seeds[k]), 0)).cuda()
+            Ai = torch.from_numpy(cu.noise_host(p.n_t, SIGMA, int(seeds[k]), 1)).cuda()
+            h = torch.zeros(inp.n_rt, dtype=torch.float64, device="cuda")
+            plan.round_trips(Ap, As, Ai, torch.from_numpy(pump).cuda(), inp.n_rt, 0, inp.n_rt, ps_hist=h)
+            torch.cuda.synchronize()
+            assert np.array_equal(As.cpu().numpy(), got[k]), k
+            assert np.array_equal(h.cpu().numpy(), hist[k]), k
+
+
+def test_rejections():
+    p, _ = cu.derive_params(cu.default_inputs(regime=cu.NS, n_t=1024, n_z=2))
+    with pytest.raises(cu.CuopoError) as e:        # base + instances cannot carry a pump window
+        cu.Batch(p, [dict(n_t=1024, ap0=p.ap0, Rs=0.98, delta=0.0, gdd=0.0, seed=0)])
     assert e.value.status == cu.EUNSUPPORTED
+    with pytest.raises(cu.CuopoError) as e:
+        cu.Batch(None, [cu.default_inputs(n_t=3000, n_z=2)])
+    assert e.value.status == cu.EINVAL
+    with cu.Batch(None, [cu.default_inputs(n_t=1024, n_z=2)]) as b, pytest.raises(cu.CuopoError):
+        b.history(0, 4)                            # CW instances keep no history
