@@ -69,7 +69,10 @@ def parse():
     ap.add_argument("--sizes", type=str, default="", help="grid sizes to draw from (default 4096,8192,16384,32768); "
                     "reduced variants are for profiling only")
     ap.add_argument("--max-rt", type=int, default=MAX_RT, help="round-trip limit (default 5000)")
-    ap.add_argument("--no-autotune", action="store_true", help="use the built-in kernel preference order")
+    ap.add_argument("--no-autotune", action="store_true", help="the default; accepted for recorded commands")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time each grid size's kernel configurations first (cuopo_autotune); default: the built-in "
+                         "order, measured on batches of every grid size running together")
     ap.add_argument("--split", action="store_true",
                     help="N > 1: split one sweep of --count instances over the ranks (strong scaling) instead of "
                          "giving every rank its own sweep (weak scaling, the default)")
@@ -293,7 +296,7 @@ def run_cuopo(args):
     # set-up (untimed): pick each grid size's kernel configuration by timing the candidates
     kernels = {}
     for n in sorted(set(int(x["n_t"]) for x in insts)):
-        if not args.no_autotune:
+        if args.autotune and not args.no_autotune:
             pb, _ = cu.derive_params(sweep.cw_base_inputs(n_t=n, n_z=N_Z))
             cu.autotune(pb, cu.F32, count=max(1, sum(1 for x in insts if x["n_t"] == n)), n_rt=2)
         m, cl = cu.kernel_config(n)
@@ -401,7 +404,7 @@ def run_cuopo(args):
                        "global_batch": args.count if split else args.count * world, "per_rank_batch": len(insts),
                        "grid_sizes": list(args.sizes), "max_rt": max_rt,
                        "round_trips_per_step": chunk, "kernels": kernels,
-                       "kernel_choice": "built-in order" if args.no_autotune else "autotuned (cuopo_autotune)",
+                       "kernel_choice": "autotuned (cuopo_autotune)" if args.autotune and not args.no_autotune else "built-in order",
                        "parallelism": (f"one sweep split over {world} ranks by expected cost" if split else
                                        f"own sweep per rank, {world} rank(s)") + ", no collective on the data path",
                        "l2": "working set (fields of 1024 instances, 252 MB) larger than L2",

@@ -1056,19 +1056,24 @@ extern "C" cuopo_status cuopo_autotune(const cuopo_params *base, int precision, 
             st = cuopo_batch_create(&b, base, inst.data(), count, precision);
             if (st == CUOPO_OK) st = cuopo_batch_seed_noise(b, 1e-15, nullptr);
             if (st == CUOPO_OK) st = cuopo_batch_run(b, 1, 0.0, 1, nullptr); /* warm-up: module load, tables */
-            if (st == CUOPO_OK) st = cuopo_batch_reset(b, nullptr);
-            float t = 0.f;
-            if (st == CUOPO_OK) {
+            /* best of two timed runs */
+            float t = -1.f;
+            for (int rep = 0; rep < 2 && st == CUOPO_OK; rep++) {
+                float ti = 0.f;
+                if ((st = cuopo_batch_reset(b, nullptr)) != CUOPO_OK) break;
                 cudaEventRecord(e0, nullptr);
                 st = cuopo_batch_step(b, n_rt, n_rt, 0.0, 1, nullptr);
                 cudaEventRecord(e1, nullptr);
                 if (st == CUOPO_OK && (e = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(e, "autotune");
-                if (st == CUOPO_OK) cudaEventElapsedTime(&t, e0, e1);
+                if (st == CUOPO_OK) cudaEventElapsedTime(&ti, e0, e1);
+                if (t < 0.f || ti < t) t = ti;
             }
             g_force = nullptr;
             if (b) cuopo_batch_destroy(b);
             if (st != CUOPO_OK) break;
-            if (best_ms < 0.0 || t < best_ms) {
+            /* the built-in choice (first candidate) stays unless another is
+             * faster by more than the run-to-run noise of such timings */
+            if (best_ms < 0.0 || t < 0.97 * best_ms) {
                 best_ms = t;
                 best = k;
             }

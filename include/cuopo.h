@@ -297,9 +297,13 @@ cuopo_status cuopo_batch_results(cuopo_batch *batch, double *ps, int *rts, int *
  * and fixed launch shapes).  Grids that more than one built kernel
  * configuration can run (e.g. 2^15 points as 8 CTAs of 4096 or 4 CTAs of
  * 8192) are timed on `count` copies of the CW 2-equation instance `base`
- * (its n_t, ap0, Rs, delta, gdd) for n_rt round trips each, and the fastest
- * becomes the one every plan and batch created afterwards in this process
- * uses for (precision, n_eqs, n_t).  Reports the chosen points per CTA,
+ * (its n_t, ap0, Rs, delta, gdd) for n_rt round trips each (best of two
+ * runs); the built-in choice stays unless another configuration is more
+ * than 3 % faster, and the result becomes the one every plan and batch
+ * created afterwards in this process uses for (precision, n_eqs, n_t).
+ * The timing runs one grid size alone: in a sweep that runs several grid
+ * sizes at once, configurations with one CTA per SM pack worse next to the
+ * others than this timing shows.  Reports the chosen points per CTA,
  * cluster size and its time (ms; -1 when there was one candidate).
  * Synchronous; allocates device memory while it runs.
  */
