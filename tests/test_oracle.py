@@ -136,3 +136,40 @@ def test_manley_rowe_three_waves():
     assert max(b) < 1e-3
     for x, y in zip(a, b):
         assert 3.0 < x / y < 5.0
+
+
+def _steady_power(n_thr, n_t=256, n_z=10):
+    p = params_2eq(n_t=n_t, n_z=n_z, n_thr=n_thr, r_percent=98.0)
+    T, w = cu.make_grids(p.n_t, p.t_rt)
+    As = np.full(n_t, 1e-2 + 0j)
+    Ap = np.zeros(n_t, np.complex128)
+    pump = np.full(n_t, np.float32(p.ap0), np.complex128)
+    rts, ps, conv = ob.solve(p, w.astype(np.float64), T.astype(np.float64), Ap, As, None, pump, 0, 20000, 1e-10)
+    return rts, ps, conv
+
+
+def test_dro_steady_state_scales_as_sqrt_pump_ratio():
+    """Above threshold the degenerate DRO's steady-state signal power grows as
+    sqrt(N) - 1 (plane-wave, non-resonant pump).  Pump ratios 1.5625, 2.25,
+    4, 6.25 give 0.5 : 1 : 2 : 3; the solver (dispersion, finite slices, the
+    reference's RK4) stays within 5 % of it (measured: 0.487, 2.023, 3.043)."""
+    ref = _steady_power(2.25)
+    assert ref[2]
+    for n_thr, ratio in ((1.5625, 0.5), (4.0, 2.0), (6.25, 3.0)):
+        rts, ps, conv = _steady_power(n_thr)
+        assert conv
+        assert abs(ps / ref[1] / ratio - 1.0) < 0.05, (n_thr, ps / ref[1])
+
+
+def test_threshold():
+    """Below threshold (N = 0.9) a seeded signal decays; above (N = 1.2) it
+    grows (measured over 1000 round trips: x0.16 and x3.4 from round trip 10)."""
+    for n_thr, grows in ((0.9, False), (1.2, True)):
+        p = params_2eq(n_t=256, n_z=10, n_thr=n_thr, r_percent=98.0)
+        T, w = cu.make_grids(p.n_t, p.t_rt)
+        As = np.full(p.n_t, 1e-4 + 0j)
+        Ap = np.zeros(p.n_t, np.complex128)
+        pump = np.full(p.n_t, np.float32(p.ap0), np.complex128)
+        ps = np.zeros(1000)
+        ob.round_trips(p, w.astype(np.float64), T.astype(np.float64), Ap, As, None, pump, 1000, 0, 1000, ps_hist=ps)
+        assert (ps[-1] > 2 * ps[10]) == grows and (ps[-1] < 0.5 * ps[10]) == (not grows), (n_thr, ps[10], ps[-1])
