@@ -361,24 +361,25 @@ def run_cuopo(args):
     clocks = ClockSampler(int(vis[local]) if local < len(vis) and vis[local].strip().isdigit() else local)
     clocks.start()
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    e_start, e_h2d, e_end = ev(), ev(), ev()
-    ks = [(ev(), ev()) for _ in range(K)]
+    e_start, e_h2d, e_steps, e_end = ev(), ev(), ev(), ev()
     torch.cuda.synchronize()
     e_start.record(stream)
     batch.set_signal(h_init)           # host -> device, pinned
     batch.reset()
     e_h2d.record(stream)
+    # the K steps: each grid size runs on its own stream and starts its next
+    # step as soon as its own part of the previous one is done
     for k in range(K):
-        ks[k][0].record(stream)
         batch.step(chunk, max_rt, TOL, 1)
-        ks[k][1].record(stream)
+    batch.wait(stream)                 # every grid size's last step done
+    e_steps.record(stream)
     ps, rts, flags = batch.results()   # device -> host (synchronises the stream)
     batch.get_signal(h_out)
     e_end.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
 
-    dev_ms = sum(a.elapsed_time(b) for a, b in ks)
+    dev_ms = e_h2d.elapsed_time(e_steps)
     e2e_ms = e_start.elapsed_time(e_end)
     done = int(np.sum(flags != 0))
     conv = int(np.sum(flags == 1))

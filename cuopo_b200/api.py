@@ -305,6 +305,10 @@ class Batch:
         else:
             check(self._lib.cuopo_batch_get_signal(self._h, dst.data_ptr(), int(dst.is_cuda), _stream(stream)))
 
+    def wait(self, stream=None) -> None:
+        """Makes `stream` wait for every grid size's queued steps."""
+        check(self._lib.cuopo_batch_wait(self._h, _stream(stream)))
+
     def history(self, i: int, n: int, stream=None) -> np.ndarray:
         """Signal power per round trip of nanosecond instance i (first n values)."""
         out = np.zeros(n)

@@ -606,6 +606,8 @@ struct cuopo_batch {
 extern "C" cuopo_status cuopo_batch_destroy(cuopo_batch *b)
 {
     if (!b) return CUOPO_OK;
+    for (BatchGroup &g : b->groups)
+        if (g.stream) cudaStreamSynchronize(g.stream);
     for (BatchGroup &g : b->groups) {
         for (cuopo_plan *pl : g.plans) cuopo_plan_destroy(pl);
         cudaFree(g.d_inst);
@@ -885,9 +887,33 @@ extern "C" cuopo_status cuopo_batch_total_elements(const cuopo_batch *b, long *n
     return CUOPO_OK;
 }
 
+/* `st` waits for the latest step of every group.  Steps do not join the
+ * caller's stream themselves: a group that finishes its part of step k
+ * starts step k+1 while larger grids still finish theirs, so the SMs a
+ * group's last wave leaves idle go to the others.  Every call that reads
+ * or writes the batch's state joins here first. */
+static cuopo_status join_groups(cuopo_batch *b, cudaStream_t st, const char *what)
+{
+    for (BatchGroup &g : b->groups) {
+        cudaError_t e = cudaStreamWaitEvent(st, g.done, 0);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+    }
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_batch_wait(cuopo_batch *b, void *stream)
+{
+    if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_wait: NULL batch");
+    return join_groups(b, (cudaStream_t)stream, "batch_wait");
+}
+
 extern "C" cuopo_status cuopo_batch_seed_noise(cuopo_batch *b, double sigma, void *stream)
 {
     if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_seed_noise: NULL batch");
+    {
+        cuopo_status js = join_groups(b, (cudaStream_t)stream, "batch_seed_noise");
+        if (js != CUOPO_OK) return js;
+    }
     if (b->precision != CUOPO_F32) return cuopo_fail(CUOPO_EUNSUPPORTED, "batch_seed_noise: F32 batches only");
     for (int i = 0; i < b->count; i++) {
         cuopo_status st = cuopo_noise_device((char *)b->d_signal + 8 * b->offset[(size_t)i], b->n_t[(size_t)i], sigma,
@@ -903,6 +929,8 @@ extern "C" cuopo_status cuopo_batch_seed_noise(cuopo_batch *b, double sigma, voi
 extern "C" cuopo_status cuopo_batch_set_signal(cuopo_batch *b, const void *src, int on_device, void *stream)
 {
     if (!b || !src) return cuopo_fail(CUOPO_EINVAL, "batch_set_signal: NULL argument");
+    cuopo_status js = join_groups(b, (cudaStream_t)stream, "batch_set_signal");
+    if (js != CUOPO_OK) return js;
     const size_t esz = b->precision == CUOPO_F32 ? 8 : 16;
     cudaError_t e = cudaMemcpyAsync(b->d_signal, src, esz * b->total,
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
@@ -913,6 +941,8 @@ extern "C" cuopo_status cuopo_batch_set_signal(cuopo_batch *b, const void *src, 
 extern "C" cuopo_status cuopo_batch_get_signal(cuopo_batch *b, void *dst, int on_device, void *stream)
 {
     if (!b || !dst) return cuopo_fail(CUOPO_EINVAL, "batch_get_signal: NULL argument");
+    cuopo_status js = join_groups(b, (cudaStream_t)stream, "batch_get_signal");
+    if (js != CUOPO_OK) return js;
     const size_t esz = b->precision == CUOPO_F32 ? 8 : 16;
     cudaError_t e = cudaMemcpyAsync(dst, b->d_signal, esz * b->total,
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
@@ -924,6 +954,8 @@ extern "C" cuopo_status cuopo_batch_reset(cuopo_batch *b, void *stream)
 {
     if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_reset: NULL batch");
     cudaStream_t st = (cudaStream_t)stream;
+    cuopo_status js = join_groups(b, st, "batch_reset");
+    if (js != CUOPO_OK) return js;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b->d_rt, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(b->d_flag, 0, sizeof(int) * b->count, st)) != cudaSuccess ||
@@ -961,7 +993,6 @@ extern "C" cuopo_status cuopo_batch_step(cuopo_batch *b, int chunk, int max_rt, 
         cuopo_status s2 = launch(g.plans[0], a, g.grid, g.stream);
         if (s2 != CUOPO_OK) return s2;
         if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess) return cuda_fail(e, "batch_step");
-        if ((e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess) return cuda_fail(e, "batch_step");
     }
     return CUOPO_OK;
 }
@@ -976,6 +1007,8 @@ extern "C" cuopo_status cuopo_batch_run(cuopo_batch *b, int max_rt, double tol, 
 extern "C" cuopo_status cuopo_batch_pending(cuopo_batch *b, int *running, void *stream)
 {
     if (!b || !running) return cuopo_fail(CUOPO_EINVAL, "batch_pending: NULL argument");
+    cuopo_status js = join_groups(b, (cudaStream_t)stream, "batch_pending");
+    if (js != CUOPO_OK) return js;
     std::vector<int> f((size_t)b->count);
     cudaError_t e = cudaMemcpyAsync(f.data(), b->d_flag, sizeof(int) * b->count, cudaMemcpyDeviceToHost,
                                     (cudaStream_t)stream);
@@ -991,6 +1024,8 @@ extern "C" cuopo_status cuopo_batch_results(cuopo_batch *b, double *ps, int *rts
 {
     if (!b) return cuopo_fail(CUOPO_EINVAL, "batch_results: NULL batch");
     cudaStream_t st = (cudaStream_t)stream;
+    cuopo_status js = join_groups(b, st, "batch_results");
+    if (js != CUOPO_OK) return js;
     cudaError_t e = cudaSuccess;
     if (ps && (e = cudaMemcpyAsync(ps, b->d_ps, sizeof(double) * b->count, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "batch_results");
@@ -1010,6 +1045,8 @@ extern "C" cuopo_status cuopo_batch_history(cuopo_batch *b, int i, double *ps, i
         return cuopo_fail(CUOPO_EINVAL, "batch_history: only nanosecond instances keep a history");
     const int m = std::min(n, b->n_rt[(size_t)i]);
     cudaStream_t st = (cudaStream_t)stream;
+    cuopo_status js = join_groups(b, st, "batch_history");
+    if (js != CUOPO_OK) return js;
     cudaError_t e = cudaMemcpyAsync(ps, b->d_hist + b->hist_off[(size_t)i], sizeof(double) * (size_t)m,
                                     cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1063,6 +1100,7 @@ extern "C" cuopo_status cuopo_autotune(const cuopo_params *base, int precision, 
                 if ((st = cuopo_batch_reset(b, nullptr)) != CUOPO_OK) break;
                 cudaEventRecord(e0, nullptr);
                 st = cuopo_batch_step(b, n_rt, n_rt, 0.0, 1, nullptr);
+                if (st == CUOPO_OK) st = cuopo_batch_wait(b, nullptr);
                 cudaEventRecord(e1, nullptr);
                 if (st == CUOPO_OK && (e = cudaEventSynchronize(e1)) != cudaSuccess) st = cuda_fail(e, "autotune");
                 if (st == CUOPO_OK) cudaEventElapsedTime(&ti, e0, e1);

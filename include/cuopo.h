@@ -285,6 +285,12 @@ cuopo_status cuopo_batch_run(cuopo_batch *batch, int max_rt, double tol, int pat
 cuopo_status cuopo_batch_reset(cuopo_batch *batch, void *stream);
 cuopo_status cuopo_batch_step(cuopo_batch *batch, int chunk, int max_rt, double tol, int patience,
                               void *stream);
+/* A step returns once its launches are queued; each grid size runs on the
+ * batch's own stream and goes on to its next step without waiting for the
+ * others (all calls below that read or write the batch's state wait for
+ * every grid size first).  cuopo_batch_wait makes `stream` wait for the
+ * work queued so far, e.g. before recording a timing event. */
+cuopo_status cuopo_batch_wait(cuopo_batch *batch, void *stream);
 /* Number of instances still running (synchronous). */
 cuopo_status cuopo_batch_pending(cuopo_batch *batch, int *running, void *stream);
 /* Per-instance last signal power, round trips run and flag (0 running,
