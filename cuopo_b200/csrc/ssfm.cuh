@@ -274,17 +274,21 @@ struct Ssfm {
         return mk<C>((R)re, (R)im);
     }
 
-    static __device__ __forceinline__ void pointwise(C (&A)[3], int n, const Ops &op, const Instance &I,
-                                                     const Tables &tab, R h6, int eom_idler, double &acc)
+    /* co0 / co1: the coefficients of op.rk0 / op.rk1, loaded once per cross
+     * pass (through a pointer they would be reloaded for every point: the
+     * shared-memory stores between points may alias it for the compiler) */
+    static __device__ __forceinline__ void pointwise(C (&A)[3], int n, const Ops &op, const C (&co0)[NCO],
+                                                     const C (&co1)[NCO], const Instance &I, const Tables &tab, R h6,
+                                                     int eom_idler, double &acc)
     {
         if (op.inject) A[0] = I.pump ? ldc<C>(I.pump, op.poff + n) : mk<C>((R)I.ap0, (R)0);
         if (op.rk0) {
-            if constexpr (F == 2) rk4_half2(A[0], A[1], op.rk0, h6);
-            else rk4_half3(A[0], A[1], A[2], op.rk0);
+            if constexpr (F == 2) rk4_half2(A[0], A[1], co0, h6);
+            else rk4_half3(A[0], A[1], A[2], co0);
         }
         if (op.rk1) {
-            if constexpr (F == 2) rk4_half2(A[0], A[1], op.rk1, h6);
-            else rk4_half3(A[0], A[1], A[2], op.rk1);
+            if constexpr (F == 2) rk4_half2(A[0], A[1], co1, h6);
+            else rk4_half3(A[0], A[1], A[2], co1);
         }
         if (op.eom) {
             const C ef = ldc<C>(tab.eom, n);
@@ -321,6 +325,12 @@ struct Ssfm {
                                                  double &acc, int t, int rank)
     {
         const C *__restrict__ twN = reinterpret_cast<const C *>(tab.twN);
+        C co0[NCO], co1[NCO];
+#pragma unroll
+        for (int k = 0; k < NCO; k++) {
+            co0[k] = op.rk0 ? ldc<C>(op.rk0, k) : mk<C>((R)0, (R)0);
+            co1[k] = op.rk1 ? ldc<C>(op.rk1, k) : mk<C>((R)0, (R)0);
+        }
 #pragma unroll 1
         for (int j = 0; j < J; j++) {
             const int n1 = rank * (M / CL) + t + j * T;
@@ -358,7 +368,7 @@ struct Ssfm {
                 C A[3];
 #pragma unroll
                 for (int f = 0; f < F; f++) A[f] = v[f][c];
-                pointwise(A, n1 + M * c, op, I, tab, h6, eom_idler, acc);
+                pointwise(A, n1 + M * c, op, co0, co1, I, tab, h6, eom_idler, acc);
 #pragma unroll
                 for (int f = 0; f < F; f++) v[f][c] = A[f];
             }
