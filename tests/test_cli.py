@@ -158,3 +158,20 @@ def test_cli_ns_three_eqs_run_matches_oracle(exe, tmp_path):
                       read_complex(tmp_path / "idler_input"))
     for name, ref in (("pump_output", sv[0]), ("signal_output", sv[1]), ("idler_output", sv[2])):
         assert rel_l2(read_complex(tmp_path / name), ref) < 5e-5, name
+
+
+@pytest.mark.gpu
+def test_cli_f64_binary_run_matches_oracle(exe, tmp_path):
+    """--f64 --format bin: FP64 fields through the executable, raw complex64
+    outputs of the saved round trips against the FP64 oracle (the outputs
+    are written as float pairs, so the bound is float rounding: 1e-6)."""
+    n_t, n_z, n_rt = 512, 6, 66
+    run(exe, ["--quiet", "--f64", "--format", "bin", "--n-t", str(n_t), "--n-z", str(n_z), "--n-rt", str(n_rt),
+              "--seed", "3", *ARGS_2EQ], tmp_path)
+    p, _ = setup_params(n_t, n_z, n_rt, ARGS_2EQ)
+    pump = np.fromfile(tmp_path / "pump_input.c64", dtype=np.complex64)
+    As0 = np.fromfile(tmp_path / "signal_input.c64", dtype=np.complex64)
+    sv = oracle_saves(p, n_rt, n_rt - 64, 64, pump, As0)
+    got = np.fromfile(tmp_path / "signal_output.c64", dtype=np.complex64)
+    assert got.shape == (64 * n_t,)
+    assert rel_l2(got, sv[1]) < 1e-6
