@@ -63,25 +63,25 @@ extern "C" const char *cuopo_version(void) { return "cuopo_b200 0.1.0 (sm_100a)"
 typedef cudaError_t (*launch_fn)(const LaunchArgs &, int clusters, cudaStream_t);
 typedef int (*occ_fn)(void);
 
-template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, int HM, int MINB>
 static cudaError_t prepare_kernel()
 {
-    using K = Ssfm<R, F, M, CL, INPLACE>;
+    using K = Ssfm<R, F, M, CL, HM>;
     static cudaError_t st = [] {
-        cudaError_t e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, INPLACE, MINB>,
+        cudaError_t e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, HM, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem_bytes());
         if (e == cudaSuccess && CL > 8)
-            e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, INPLACE, MINB>,
+            e = cudaFuncSetAttribute(ssfm_kernel<R, F, M, CL, HM, MINB>,
                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         return e;
     }();
     return st;
 }
 
-template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, int HM, int MINB>
 static cudaLaunchConfig_t make_config(int clusters, cudaStream_t st, cudaLaunchAttribute *attr)
 {
-    using K = Ssfm<R, F, M, CL, INPLACE>;
+    using K = Ssfm<R, F, M, CL, HM>;
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3((unsigned)(clusters * CL));
@@ -97,49 +97,51 @@ static cudaLaunchConfig_t make_config(int clusters, cudaStream_t st, cudaLaunchA
     return cfg;
 }
 
-template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, int HM, int MINB>
 static cudaError_t launch_impl(const LaunchArgs &a, int clusters, cudaStream_t st)
 {
-    cudaError_t e = prepare_kernel<R, F, M, CL, INPLACE, MINB>();
+    cudaError_t e = prepare_kernel<R, F, M, CL, HM, MINB>();
     if (e != cudaSuccess) return e;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, INPLACE, MINB>(clusters, st, attr);
-    e = cudaLaunchKernelEx(&cfg, ssfm_kernel<R, F, M, CL, INPLACE, MINB>, a);
+    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, HM, MINB>(clusters, st, attr);
+    e = cudaLaunchKernelEx(&cfg, ssfm_kernel<R, F, M, CL, HM, MINB>, a);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
 /* Clusters (of CL CTAs) of this kernel that can be resident at once (0 on error). */
-template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, int HM, int MINB>
 static int occupancy_impl()
 {
-    if (prepare_kernel<R, F, M, CL, INPLACE, MINB>() != cudaSuccess) return 0;
+    if (prepare_kernel<R, F, M, CL, HM, MINB>() != cudaSuccess) return 0;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, INPLACE, MINB>(1, 0, attr);
+    cudaLaunchConfig_t cfg = make_config<R, F, M, CL, HM, MINB>(1, 0, attr);
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, ssfm_kernel<R, F, M, CL, INPLACE, MINB>, &cfg) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveClusters(&n, ssfm_kernel<R, F, M, CL, HM, MINB>, &cfg) != cudaSuccess) return 0;
     return n;
 }
 
 struct KernelEntry {
     int precision, F, M, CL;
-    bool inplace;
+    int home; /* 0, 1: fields in shared memory (1: in place); 2: in global memory */
     size_t smem;
     launch_fn fn;
     occ_fn occ;
 };
 
-#define CUOPO_K(R, PREC, F, M, CL, IP, MINB)                                                  \
-    {PREC, F, M, CL, IP, Ssfm<R, F, M, CL, IP>::smem_bytes(), &launch_impl<R, F, M, CL, IP, MINB>, \
-     &occupancy_impl<R, F, M, CL, IP, MINB>}
+#define CUOPO_K(R, PREC, F, M, CL, HM, MINB)                                                  \
+    {PREC, F, M, CL, HM, Ssfm<R, F, M, CL, HM>::smem_bytes(), &launch_impl<R, F, M, CL, HM, MINB>, \
+     &occupancy_impl<R, F, M, CL, HM, MINB>}
 
-/* Built configurations.  Where a grid size has more than one, cuopo_autotune
- * times them and records the winner; without a recorded choice the first
- * entry with M * CL == n_t is used (the entries are in order of measured batch
- * throughput on the B200: 2-eq 2^13, 2^14 and 2^15 run faster as clusters of
- * 2, 4 and 8 4096-point CTAs, two CTAs per SM, than as 1, 2 and 4 8192-point
- * CTAs, one per SM).  The single-CTA entries stay reachable for callers that
- * need one (crystal_pass_noalloc). */
+/* Built configurations (R, precision, equations, points per CTA, CTAs per
+ * cluster, field placement as Ssfm's HM, minimum CTAs per SM).  Where a grid
+ * size has more than one, cuopo_autotune times them and records the winner;
+ * without a recorded choice the first entry with M * CL == n_t is used (the
+ * entries are in order of measured batch throughput on the B200: 2-eq 2^13,
+ * 2^14 and 2^15 run faster as clusters of 2, 4 and 8 4096-point CTAs, two
+ * CTAs per SM, than as 1, 2 and 4 8192-point CTAs, one per SM).  The
+ * single-CTA entries stay reachable for callers that need one
+ * (crystal_pass_noalloc). */
 static const KernelEntry k_kernels[] = {
     CUOPO_K(float, CUOPO_F32, 2, 512, 1, false, 1),
     CUOPO_K(float, CUOPO_F32, 2, 1024, 1, false, 1),
@@ -168,12 +170,18 @@ static const KernelEntry k_kernels[] = {
     CUOPO_K(double, CUOPO_F64, 2, 4096, 2, false, 1),
     CUOPO_K(double, CUOPO_F64, 2, 4096, 4, false, 1),
     CUOPO_K(double, CUOPO_F64, 2, 4096, 8, false, 1),
+    CUOPO_K(double, CUOPO_F64, 2, 4096, 16, false, 1),
     CUOPO_K(double, CUOPO_F64, 3, 512, 1, false, 1),
     CUOPO_K(double, CUOPO_F64, 3, 1024, 1, false, 1),
     CUOPO_K(double, CUOPO_F64, 3, 2048, 1, false, 1),
     CUOPO_K(double, CUOPO_F64, 3, 4096, 1, true, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 4096, 2, true, 1),
     CUOPO_K(double, CUOPO_F64, 3, 2048, 8, false, 1),
+    CUOPO_K(double, CUOPO_F64, 3, 4096, 8, true, 1),
     CUOPO_K(double, CUOPO_F64, 3, 4096, 16, true, 1),
+    /* 2^17 FP64 points of 3 fields (6 MiB) exceed the shared memory of a
+     * 16-CTA cluster: the fields stay in global memory (L2) */
+    CUOPO_K(double, CUOPO_F64, 3, 8192, 16, 2, 1),
 };
 
 /* Autotuned choices, process-wide: (precision, F, N) -> entry. */

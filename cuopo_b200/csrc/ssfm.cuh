@@ -174,8 +174,19 @@ __device__ __forceinline__ void rk4_half3(C &Ap, C &As, C &Ai, const C *__restri
 
 namespace cg = cooperative_groups;
 
-template <typename R, int F, int M, int CL, bool INPLACE>
+/* Where the fields live during a launch (HM):
+ *   0  shared memory: home[F][M] and a scratch[M] for the local transforms
+ *   1  shared memory, in place: home[F][M], the local transforms exchange
+ *      through the field's own home
+ *   2  global memory: the caller's field buffers, L2-resident between
+ *      passes, with one shared scratch[M] for the local transforms; for grids
+ *      whose fields exceed a cluster's shared memory (3 FP64 fields of 2^17
+ *      points are 6 MiB, a 16-CTA cluster has 3.6 MB).  Every access to
+ *      the fields goes to L2 (ld/st .cg), ordered by the cluster barriers. */
+template <typename R, int F, int M, int CL, int HM>
 struct Ssfm {
+    static constexpr bool GH = (HM == 2);
+    static constexpr bool INPLACE = (HM != 0); /* one exchange buffer per local transform */
     using C = cpx<R>;
     using SP = StagePlan<M>;
     static constexpr int T = SP::T;
@@ -186,9 +197,9 @@ struct Ssfm {
     static constexpr unsigned ALL = (1u << F) - 1u;
     static_assert(CL == 1 || CL == 2 || CL == 4 || CL == 8 || CL == 16, "cluster size must be 1..16, power of 2");
 
-    /* Shared memory: home[F][M] (+ scratch[M]) complex values, then the
-     * twiddle table of the middle FFT stages. */
-    static constexpr size_t field_elems() { return (size_t)M * (F + (INPLACE ? 0 : 1)); }
+    /* Shared memory: home[F][M] (+ scratch[M]) complex values, or scratch[M]
+     * alone (HM = 2), then the twiddle table of the middle FFT stages. */
+    static constexpr size_t field_elems() { return GH ? (size_t)M : (size_t)M * (F + (INPLACE ? 0 : 1)); }
     static constexpr size_t smem_bytes() { return sizeof(C) * (field_elems() + TwTable<M>::size()); }
 
     /* Element-wise work of one cross stage (uniform over the cluster). */
@@ -251,7 +262,14 @@ struct Ssfm {
 
     static __device__ __forceinline__ void xsync()
     {
-        if constexpr (CL > 1) cg::this_cluster().sync();
+        if constexpr (GH) {
+            /* the cross passes write other CTAs' positions of global memory */
+            __threadfence();
+            if constexpr (CL > 1) cg::this_cluster().sync();
+            else __syncthreads();
+        } else if constexpr (CL > 1) {
+            cg::this_cluster().sync();
+        }
     }
 
     static __device__ __forceinline__ void bar()
@@ -315,15 +333,91 @@ struct Ssfm {
         if (op.power) acc += cabs2d(A[1]);
     }
 
+    /* The radix-CL stage of one field at the owned position n1 (S = -1: the
+     * inverse cross stage, y -> time; S = +1: the forward one), on global
+     * memory. */
+    template <int S>
+    static __device__ __forceinline__ void cross_field(C *g, const C *__restrict__ twN, int n1)
+    {
+        C v[CL];
+#pragma unroll
+        for (int c = 0; c < CL; c++) v[c] = __ldcg(g + (size_t)c * M + n1);
+        if constexpr (S < 0) {
+#pragma unroll
+            for (int c = 1; c < CL; c++) {
+                const long q = (long)n1 * c;
+                const C w = __ldg(twN + q);
+                v[c] = shear_rot(iq_rt(v[c], (-(int)(((4 * q + N / 2) / N) & 3)) & 3), -w.x, -w.y);
+            }
+            dft<-1, CL>(v);
+        } else {
+            dft<+1, CL>(v);
+#pragma unroll
+            for (int c = 1; c < CL; c++) {
+                const long q = (long)n1 * c;
+                const C w = __ldg(twN + q);
+                v[c] = shear_rot(iq_rt(v[c], (int)(((4 * q + N / 2) / N) & 3)), w.x, w.y);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CL; c++) __stcg(g + (size_t)c * M + n1, v[c]);
+    }
+
+    /* The element-wise pass of `cross` with the fields in global memory
+     * (HM = 2): the same arithmetic in the same order, but one field's
+     * radix-CL stage at a time, the intermediate values going through L2 (CL
+     * values of 3 FP64 fields would not fit in registers).  Thread t still
+     * reads and writes only its own positions, so these steps need no
+     * barrier between them. */
+    static __device__ __forceinline__ void cross_global(C *const (&gf)[3], unsigned in_y, unsigned out_y,
+                                                        const Ops &op, const Instance &I, const Tables &tab, R h6,
+                                                        int eom_idler, double &acc, int t, int rank)
+    {
+        const C *__restrict__ twN = reinterpret_cast<const C *>(tab.twN);
+        C co0[NCO], co1[NCO];
+#pragma unroll
+        for (int k = 0; k < NCO; k++) {
+            co0[k] = op.rk0 ? ldc<C>(op.rk0, k) : mk<C>((R)0, (R)0);
+            co1[k] = op.rk1 ? ldc<C>(op.rk1, k) : mk<C>((R)0, (R)0);
+        }
+#pragma unroll 1
+        for (int j = 0; j < J; j++) {
+            const int n1 = rank * (M / CL) + t + j * T;
+            if constexpr (CL > 1) {
+#pragma unroll 1
+                for (int f = 0; f < F; f++)
+                    if ((in_y >> f) & 1u) cross_field<-1>(gf[f], twN, n1);
+            }
+#pragma unroll 2
+            for (int c = 0; c < CL; c++) {
+                C A[3];
+#pragma unroll
+                for (int f = 0; f < F; f++) A[f] = __ldcg(gf[f] + (size_t)c * M + n1);
+                pointwise(A, n1 + M * c, op, co0, co1, I, tab, h6, eom_idler, acc);
+#pragma unroll
+                for (int f = 0; f < F; f++) __stcg(gf[f] + (size_t)c * M + n1, A[f]);
+            }
+            if constexpr (CL > 1) {
+#pragma unroll 1
+                for (int f = 0; f < F; f++)
+                    if ((out_y >> f) & 1u) cross_field<+1>(gf[f], twN, n1);
+            }
+        }
+    }
+
     /* One element-wise pass over the cluster.  Fields with their bit set in
      * in_y are read in the y domain (inverse cross stage applied), the
      * others as time values; out_y likewise for the write-back.  Thread t
      * of CTA `rank` owns positions n1 = rank M/CL + t + j T, j < J, in every
      * CTA's home; it reads and writes only those. */
-    static __device__ __forceinline__ void cross(C *home, unsigned in_y, unsigned out_y, const Ops &op,
-                                                 const Instance &I, const Tables &tab, R h6, int eom_idler,
-                                                 double &acc, int t, int rank)
+    static __device__ __forceinline__ void cross(C *home, C *const (&gf)[3], unsigned in_y, unsigned out_y,
+                                                 const Ops &op, const Instance &I, const Tables &tab, R h6,
+                                                 int eom_idler, double &acc, int t, int rank)
     {
+        if constexpr (GH) {
+            cross_global(gf, in_y, out_y, op, I, tab, h6, eom_idler, acc, t, rank);
+            return;
+        }
         const C *__restrict__ twN = reinterpret_cast<const C *>(tab.twN);
         C co0[NCO], co1[NCO];
 #pragma unroll
@@ -399,9 +493,15 @@ struct Ssfm {
                                                     int t)
     {
         C reg[16];
-        load_own<M>(home, reg, t);
-        C *bufA = INPLACE ? home : scratch;
-        C *bufB = home;
+        if constexpr (GH) {
+            /* home: this CTA's M points of the field in global memory */
+#pragma unroll
+            for (int e = 0; e < 16; e++) reg[e] = __ldcg(home + t + e * T);
+        } else {
+            load_own<M>(home, reg, t);
+        }
+        C *bufA = GH ? scratch : (INPLACE ? home : scratch);
+        C *bufB = GH ? scratch : home;
         local_transform<+1, M, 0, INPLACE>(reg, bufA, bufB, tw, t);
         /* the factor F = 1 + d is applied as (A + A d) / N (1/N is exact) */
         const R s_n = (R)inv_n;
@@ -426,7 +526,12 @@ struct Ssfm {
             }
         }
         local_transform<-1, M, P - 1, INPLACE>(reg, bufA, bufB, tw, t);
-        store_own<M>(home, reg, t);
+        if constexpr (GH) {
+#pragma unroll
+            for (int e = 0; e < 16; e++) __stcg(home + t + e * T, reg[e]);
+        } else {
+            store_own<M>(home, reg, t);
+        }
     }
 
     static __device__ __forceinline__ double block_sum(double v, double *red, int t)
@@ -445,8 +550,9 @@ struct Ssfm {
     static __device__ __forceinline__ void run(const LaunchArgs &a)
     {
         extern __shared__ __align__(16) unsigned char smem_raw[];
-        C *home = reinterpret_cast<C *>(smem_raw);
-        C *scratch = INPLACE ? home : home + (size_t)F * M;
+        C *const sm = reinterpret_cast<C *>(smem_raw);
+        C *home = GH ? nullptr : sm;
+        C *scratch = GH ? sm : (INPLACE ? home : home + (size_t)F * M);
         __shared__ double red[32];
         __shared__ double red_cl;
         __shared__ int next_inst;
@@ -454,7 +560,7 @@ struct Ssfm {
         int rank = 0;
         if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
 
-        C *twtab = home + field_elems();
+        C *twtab = sm + field_elems();
         fill_twiddle_table<M>(twtab, t);
         StageTwiddles<M, C> tw;
         tw.init(t, twtab);
@@ -503,12 +609,17 @@ struct Ssfm {
                 patience = a.patience;
             }
 
-            C *gf[3] = {reinterpret_cast<C *>(I.Ap), reinterpret_cast<C *>(I.As), reinterpret_cast<C *>(I.Ai)};
+            C *const gf[3] = {reinterpret_cast<C *>(I.Ap), reinterpret_cast<C *>(I.As),
+                              reinterpret_cast<C *>(I.Ai)};
+            /* the field f of this CTA for the local transforms */
+            auto fld = [&](int f) -> C * { return GH ? gf[f] + (size_t)rank * M : home + (size_t)f * M; };
+            if constexpr (!GH) {
 #pragma unroll
-            for (int f = 0; f < F; f++)
+                for (int f = 0; f < F; f++)
 #pragma unroll
-                for (int e = 0; e < 16; e++)
-                    home[f * M + swz<C>(t + e * T)] = gf[f][(size_t)rank * M + t + e * T];
+                    for (int e = 0; e < 16; e++)
+                        home[f * M + swz<C>(t + e * T)] = gf[f][(size_t)rank * M + t + e * T];
+            }
             xsync();
 
             double ps = prev_ps, acc = 0.0;
@@ -527,21 +638,21 @@ struct Ssfm {
                     }
                     op.rk0 = rk;
                     frame_step(op, tab, frame_index(rt, 0), th);
-                    cross(home, 0u, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    cross(home, gf, 0u, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
                 }
                 for (int s = 0; s < a.n_z; s++) {
 #pragma unroll 1
                     for (int f = 0; f < F; f++)
-                        spectral<0>(home + f * M, scratch, disp + ((size_t)f * CL + rank) * M, nullptr, 0.0, 0.0,
-                                    0, tab.inv_n, tw, t);
+                        spectral<0>(fld(f), scratch, disp + ((size_t)f * CL + rank) * M, nullptr, 0.0, 0.0, 0,
+                                    tab.inv_n, tw, t);
                     xsync();
                     if (s + 1 < a.n_z) {
                         Ops op{};
                         op.rk0 = rk + (size_t)s * NCO;
                         op.rk1 = rk + (size_t)(s + 1) * NCO;
                         frame_step(op, tab, frame_index(rt, s + 1), th);
-                        cross(home, ALL, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                        cross(home, gf, ALL, ALL, op, I, tab, h6, a.eom_idler, acc, t, rank);
                         xsync();
                     }
                 }
@@ -550,7 +661,7 @@ struct Ssfm {
                     Ops op{};
                     op.rk0 = last_row;
                     frame_back(op, th);
-                    cross(home, ALL, 0u, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    cross(home, gf, ALL, 0u, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
                     break;
                 }
@@ -570,20 +681,19 @@ struct Ssfm {
                     op.rk0 = last_row;
                     op.eom = use_eom;
                     const unsigned res = ALL & ~1u;
-                    cross(home, ALL, res, op, I, tab, h6, a.eom_idler, acc, t, rank);
+                    cross(home, gf, ALL, res, op, I, tab, h6, a.eom_idler, acc, t, rank);
                     xsync();
-                    spectral<1>(home + 1 * M, scratch, nullptr, wtab, I.gdd, I.tod_s, I.use_tod_s, tab.inv_n, tw, t);
+                    spectral<1>(fld(1), scratch, nullptr, wtab, I.gdd, I.tod_s, I.use_tod_s, tab.inv_n, tw, t);
                     if constexpr (F == 3)
-                        spectral<1>(home + 2 * M, scratch, nullptr, wtab, I.gdd, I.tod_i, I.use_tod_i, tab.inv_n, tw,
-                                    t);
+                        spectral<1>(fld(2), scratch, nullptr, wtab, I.gdd, I.tod_i, I.use_tod_i, tab.inv_n, tw, t);
                     xsync();
                     frame_back(end, th);
-                    cross(home, res, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
+                    cross(home, gf, res, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 } else {
                     end.rk0 = last_row;
                     end.eom = use_eom;
                     frame_back(end, th);
-                    cross(home, ALL, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
+                    cross(home, gf, ALL, 0u, end, I, tab, h6, a.eom_idler, acc, t, rank);
                 }
                 /* signal power over the cluster, summed in rank order by every CTA */
                 double part = block_sum(acc, red, t);
@@ -614,11 +724,13 @@ struct Ssfm {
                 }
                 prev_ps = ps;
             }
+            if constexpr (!GH) {
 #pragma unroll
-            for (int f = 0; f < F; f++)
+                for (int f = 0; f < F; f++)
 #pragma unroll
-                for (int e = 0; e < 16; e++)
-                    gf[f][(size_t)rank * M + t + e * T] = home[f * M + swz<C>(t + e * T)];
+                    for (int e = 0; e < 16; e++)
+                        gf[f][(size_t)rank * M + t + e * T] = home[f * M + swz<C>(t + e * T)];
+            }
             if (rank == 0 && t == 0) {
                 if (I.rt_done) *I.rt_done = rts;
                 if (I.ps_out) *I.ps_out = ps;
@@ -635,10 +747,10 @@ struct Ssfm {
     }
 };
 
-template <typename R, int F, int M, int CL, bool INPLACE, int MINB>
+template <typename R, int F, int M, int CL, int HM, int MINB>
 __global__ void __launch_bounds__(M / 16, MINB) ssfm_kernel(const LaunchArgs a)
 {
-    Ssfm<R, F, M, CL, INPLACE>::run(a);
+    Ssfm<R, F, M, CL, HM>::run(a);
 }
 
 }  // namespace cuopo

@@ -170,6 +170,8 @@ typedef struct cuopo_plan cuopo_plan;
  * EvolutionInCrystal as w_ext_gpu (cuOPO.cu:183-189); NULL = build them
  * with cuopo_make_grids.  T_host likewise (used by the modulator).
  * Replaces the set-up of cuOPO.cu:379-454 (buffers, cufftPlan1d).
+ * Grids (n_t, powers of 2): F32 512..2^16 with 2 equations, 512..2^17 with
+ * 3; F64 512..2^16 with 2, 512..2^17 with 3.  Other sizes: CUOPO_EUNSUPPORTED.
  */
 cuopo_status cuopo_plan_create(cuopo_plan **plan, const cuopo_params *p,
                                const float *w_host, const float *T_host,

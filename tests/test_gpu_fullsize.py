@@ -12,6 +12,9 @@ tests/test_gpu_ssfm.py; the CPU oracle itself would need hours here.)
   Gaussian pump at 3x threshold, 2^16 points, 200 slices, 600 round trips,
   group-velocity mismatch, dispersion and absorption on, 1e-15 noise
   (seed 1); fields saved around the pump peak.
+* precision study: the same OPO at 2^17 points, 400 slices, 1000 round
+  trips (the FP64 run keeps its fields in global memory: 3 FP64 fields of
+  2^17 points exceed a cluster's shared memory).
 
 Tolerances (measured values on the B200 in brackets): signal power per
 round trip 1e-4 [3e-5], output energy 1e-5 [8e-7].  Fields are compared
@@ -24,7 +27,11 @@ per-mode amplitude error of ~1e-8 x 2e5 slices, while the power, carried
 by the low-frequency modes where |d| ~ 1e-4, stays within 3e-5.  The
 nanosecond signal and idler stay at the noise level (the 10 ns pump lasts
 ~25 of the 600 round trips), so the same per-mode effect over 6e4 slices
-sets their bound: 1e-2 [2.1e-3]; the pump 1e-3.
+sets their bound: 1e-2 [2.1e-3]; the pump 1e-3.  The precision study
+(2^17, 4e5 slices): output energy 1e-4 [2.3e-5], signal power per round
+trip 2e-3 [5.9e-4], signal and idler 3e-2 [7.8e-3, 9.6e-3], pump 1e-3
+[3.2e-6] -- twice the bandwidth puts a larger share of the noise power
+into the high-frequency modes with |d| ~ 1, over 3.3 times the slices.
 """
 import numpy as np
 import pytest
@@ -80,9 +87,13 @@ def test_single_cw_opo_2000_round_trips():
     assert e_s < 2e-2, e_s
 
 
-def test_nanosecond_three_wave_opo_600_round_trips():
-    n_t, n_rt = 65536, 600
-    inp = cu.default_inputs(crystal=cu.SPPLT, n_eqs=3, regime=cu.NS, n_t=n_t, n_z=200, n_rt=n_rt, lp_nm=532.0,
+# bounds: (output energy, signal power per round trip, pump field, signal and idler fields)
+NS_BOUNDS = {65536: (1e-5, 1e-4, 1e-3, 1e-2), 131072: (1e-4, 2e-3, 1e-3, 3e-2)}
+
+
+@pytest.mark.parametrize("n_t,n_z,n_rt", [(65536, 200, 600), (131072, 400, 1000)])
+def test_nanosecond_three_wave_opo(n_t, n_z, n_rt):
+    inp = cu.default_inputs(crystal=cu.SPPLT, n_eqs=3, regime=cu.NS, n_t=n_t, n_z=n_z, n_rt=n_rt, lp_nm=532.0,
                             ls_nm=1550.0, lambda_um=8.719670871908674, n_thr=3.0, r_percent=98.0, lcr_mm=20.0)
     p, _ = cu.derive_params(inp)
     As = cu.noise_host(n_t, 1e-15, 1, 1).astype(np.complex128)
@@ -93,14 +104,17 @@ def test_nanosecond_three_wave_opo_600_round_trips():
     a = run(p, cu.F32, zero, f32(As), f32(Ai), f32(pump), n_rt, sf, sc)
     b = run(p, cu.F64, zero, As, Ai, pump, n_rt, sf, sc)
     e_energy = abs(a[1].sum() - b[1].sum()) / b[1].sum()
-    assert e_energy < 1e-5, e_energy
     e_ps = np.max(np.abs(a[1] - b[1]) / b[1])
-    assert e_ps < 1e-4, e_ps
     errs = {}
     for f, name in enumerate(("pump", "signal", "idler")):
         for r in (0, sc // 2, sc - 1):
             x = a[2][f][r * n_t:(r + 1) * n_t]
             y = b[2][f][r * n_t:(r + 1) * n_t]
             errs[(name, sf + r)] = aligned_rel(x, y)
-    bad = {k: e for k, e in errs.items() if e > (1e-3 if k[0] == "pump" else 1e-2)}
+    print(f"n_t={n_t}: energy {e_energy:.2e}, signal power per rt {e_ps:.2e}, fields",
+          {f"{k[0]}@{k[1]}": f"{e:.1e}" for k, e in errs.items()})
+    b_energy, b_ps, b_pump, b_field = NS_BOUNDS[n_t]
+    assert e_energy < b_energy, e_energy
+    assert e_ps < b_ps, e_ps
+    bad = {k: e for k, e in errs.items() if e > (b_pump if k[0] == "pump" else b_field)}
     assert not bad, errs

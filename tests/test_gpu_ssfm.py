@@ -58,9 +58,11 @@ def run_pass_oracle(p, Ap, As, Ai):
     return A
 
 
-# single-CTA grids and cluster grids (2-16 CTAs with distributed shared memory)
+# single-CTA grids and cluster grids (2-16 CTAs with distributed shared memory;
+# FP64 3-eq 2^17: fields in global memory)
 CASES_F64 = [(2, 512), (2, 1024), (2, 2048), (2, 4096), (3, 512), (3, 1024), (3, 2048), (3, 4096),
-             (2, 8192), (2, 16384), (2, 32768), (3, 16384), (3, 65536)]
+             (2, 8192), (2, 16384), (2, 32768), (2, 65536), (3, 8192), (3, 16384), (3, 32768), (3, 65536),
+             (3, 131072)]
 CASES_F32 = [(2, 512), (2, 1024), (2, 2048), (2, 4096), (2, 8192), (3, 512), (3, 1024), (3, 2048), (3, 4096),
              (3, 8192), (2, 16384), (2, 32768), (2, 65536), (3, 16384), (3, 32768), (3, 65536), (3, 131072)]
 
@@ -134,6 +136,7 @@ RT_CASES = [
     (2, 16384, cu.CW, dict(delta=0.03, gdd_percent=30.0, use_eom=1)),
     (2, 32768, cu.CW, dict(r_percent=95.0)),
     (3, 65536, cu.NS, dict(gdd_percent=20.0)),
+    (3, 131072, cu.NS, dict(gdd_percent=20.0, use_eom=1, mod_depth_pi=0.6, freq_det_mhz=4.0)),
 ]
 
 
