@@ -19,8 +19,10 @@ steps; e2e adds the host->device copy of the initial fields from pinned
 memory and the device->host read of every instance's result and field.
 
 --impl reference times the reference's own crystal-pass code and cuFFT
-(oracle/_ref, compiled from the reference's sources) on a bounded sample:
-K steps of a few round trips of one sweep instance per grid size, scaled to
+(oracle/_ref, compiled from the reference's sources; its parameters, grids
+and pump from the reference's own set-up code in the same library, without
+this package) on a bounded sample: every step runs 20 round trips of one
+sweep instance per grid size, and the mean time per round trip is scaled to
 the sweep by the round trips each instance needs (tests/golden).
 
 Launch: python bench.py [--gpus N --steps K --warmup W]; N > 1 under
@@ -51,6 +53,8 @@ TOL = 1e-7
 N_Z = 100
 NOISE = 1e-15
 SIZES = (4096, 8192, 16384, 32768)
+LAMBDA_UM = 6.970206862971646   # QPM period: dk = 0 at 26.85 C for 532 -> 1064 nm in MgO:PPLN
+REF_RTS_PER_STEP = 20
 RTS_RECORD = ROOT / "tests" / "golden" / "cw_sweep_rts.json"
 TRAFFIC_RECORD = ROOT / "profiles" / "ssfm_traffic.json"
 CPU_RTS = 4
@@ -201,7 +205,40 @@ def cpu_baseline_leg(insts, rts_by_size):
             "sample": f"{CPU_RTS} round trips of one sweep instance per grid size in each of {cores} processes at "
                       f"once (FP32 C restatement, radix-2 FFT, {wall:.1f} s wall), scaled by the sweep's round trips "
                       f"per grid size and divided over the cores",
-            "s_per_rt": {str(k): round(v, 4) for k, v in per_rt.items()}}
+            "s_per_rt": {str(k): round(v, 4) for k, v in per_rt.items()},
+            "single_cw_opo_1core": single_cw_opo_cpu(), "cpu_model": cpu_model(), "nproc": os.cpu_count()}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def single_cw_opo_cpu(n_rt_sample: int = 3) -> dict:
+    """The single CW OPO (2-eq MgO:PPLN, 2^13 points, 100 slices, N = 4,
+    R = 0.98, 2000 round trips) on one host core with the C restatement, in
+    FP64 and FP32: a few round trips timed, scaled to the 2000 of a run."""
+    import cuopo_b200 as cu
+    from cuopo_b200 import sweep
+    from oracle import binding as ob
+    p, _ = cu.derive_params(sweep.cw_base_inputs(n_t=8192, n_z=N_Z))
+    T, w = cu.make_grids(p.n_t, p.t_rt)
+    out = {}
+    for bits, ct in ((64, np.complex128), (32, np.complex64)):
+        As = cu.noise_host(p.n_t, 1e-20, 0).astype(ct)
+        Ap = np.zeros(p.n_t, ct)
+        pump = cu.pump_cw(p.n_t, p.ap0).astype(ct)
+        t0 = time.perf_counter()
+        ob.round_trips(p, w, T, Ap, As, None, pump, 0, 0, n_rt_sample, bits=bits)
+        s_rt = (time.perf_counter() - t0) / n_rt_sample
+        out[f"fp{bits}"] = {"s_per_rt": round(s_rt, 4), "s_per_run_2000_rt": round(2000 * s_rt, 1)}
+    out["sample"] = f"{n_rt_sample} round trips per precision on 1 core (radix-2 C FFT; FFTW3 is not installed)"
+    return out
 
 
 def load_rts_record(count):
@@ -220,10 +257,23 @@ def rts_by_size_from(rec, table):
     return out
 
 
+def draw_sweep_table(count: int, rng_seed: int, sizes=SIZES) -> dict:
+    """The batched CW sweep's parameter draws: the generator calls of
+    cuopo_b200.sweep.random_cw_sweep, repeated here so that the reference arm
+    draws the same instances without importing this package."""
+    rng = np.random.default_rng(rng_seed)
+    N = rng.uniform(1.2, 6.0, count)
+    dl = rng.uniform(-np.pi, np.pi, count)
+    gd = rng.uniform(-500.0, 500.0, count)
+    R = rng.uniform(0.90, 0.99, count)
+    nt = rng.choice(np.asarray(sizes), count)
+    return dict(n_thr=N, delta_rad=dl, gdd_fs2=gd, refl=R, n_t=nt)
+
+
 def run_reference(args):
-    """The reference arm: its own kernels + cuFFT (oracle/_ref) on a bounded sample."""
-    import cuopo_b200 as cu
-    from cuopo_b200 import sweep
+    """The reference arm: its own kernels + cuFFT (oracle/_ref) on a bounded
+    sample, set up by its own host code (ref_setup_cw2); imports nothing of
+    this package, so only oracle/_ref libraries are loaded."""
     from oracle import binding as ob
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -236,24 +286,26 @@ def run_reference(args):
         line["unavailable"] = f"reference harness not built for grid sizes {missing} (oracle/build_ref.sh)"
         print(json.dumps(line))
         return 0
-    base, insts, table = sweep.random_cw_sweep(args.count, 0, n_t_choices=SIZES, n_z=N_Z)
+    table = draw_sweep_table(args.count, 0)
     rec = load_rts_record(args.count)
     rts_by_size = rts_by_size_from(rec, table) if rec else {n: MAX_RT * int(np.sum(table["n_t"] == n)) for n in SIZES}
     sample = {}
     for n_t in SIZES:
-        k = next(i for i, x in enumerate(insts) if x["n_t"] == n_t)
-        p, _ = cu.derive_params(sweep.cw_base_inputs(n_t=n_t, n_z=N_Z))
-        p.Rs, p.delta, p.gdd, p.ap0 = insts[k]["Rs"], insts[k]["delta"], insts[k]["gdd"], insts[k]["ap0"]
-        T, w = cu.make_grids(n_t, p.t_rt)
-        sample[n_t] = (p, w, T, cu.pump_cw(n_t, p.ap0), cu.noise_host(n_t, NOISE, insts[k]["seed"]))
-    rts_per_step = 3
+        k = int(np.flatnonzero(table["n_t"] == n_t)[0])
+        rp, w, T, pump, _, _ = ob.ref_setup_cw2(n_t, 532.0, LAMBDA_UM, float(table["n_thr"][k]),
+                                                float(table["refl"][k]) * 100.0,
+                                                float(table["delta_rad"][k]) / np.pi,
+                                                float(table["gdd_fs2"][k]) * 1e-6, 5.0, N_Z)
+        rng = np.random.default_rng(k)
+        As0 = (NOISE * (rng.standard_normal(n_t) + 1j * rng.standard_normal(n_t))).astype(np.complex64)
+        sample[n_t] = (rp, w, T, pump, As0)
 
     def one_step():
         ms = {}
-        for n_t, (p, w, T, pump, As0) in sample.items():
+        for n_t, (rp, w, T, pump, As0) in sample.items():
             Ap, As = pump.copy(), As0.copy()
-            _, t = ob.ref_round_trips("ppln", p, w, T, Ap, As, None, pump, 0, 0, rts_per_step)
-            ms[n_t] = t / rts_per_step
+            _, t = ob.ref_round_trips("ppln", rp, w, T, Ap, As, None, pump, 0, 0, REF_RTS_PER_STEP)
+            ms[n_t] = t / REF_RTS_PER_STEP
         return ms
 
     for _ in range(args.warmup):
@@ -267,19 +319,31 @@ def run_reference(args):
         for n in SIZES:
             acc[n].append(ms[n])
     ms_rt = {n: float(np.mean(acc[n])) for n in SIZES}
+    per_step_value = [args.count / sum(rts_by_size[n] * acc[n][k] * 1e-3 for n in SIZES) for k in range(args.steps)]
     est_s = sum(rts_by_size[n] * ms_rt[n] * 1e-3 for n in SIZES)
     value = args.count / est_s
+    converged = int(np.sum(np.asarray(rec["flags"]) == 1)) if rec else None
     line.update({
         "value": value, "ms_per_step": 1e3 * float(np.mean(t_steps)),
+        "converged_solves_per_s": (converged / est_s) if converged is not None else None,
         "config": {"workload": "batched CW sweep, 1024 instances (2-eq MgO:PPLN, N~U[1.2,6], delta~U[-pi,pi], "
                                "GDD~U[-500,500] fs^2, R~U[0.90,0.99], grid 2^12..2^15, 100 slices, tol 1e-7, "
                                "max 5000 rt), reference kernels + cuFFT run one instance at a time",
-                   "global_batch": args.count, "sample": f"{rts_per_step} round trips per grid size per step",
+                   "global_batch": args.count,
+                   "sample": f"{REF_RTS_PER_STEP} round trips of one sweep instance per grid size per step",
                    "ms_per_round_trip": {str(n): round(ms_rt[n], 3) for n in SIZES},
-                   "round_trips_source": "tests/golden/cw_sweep_rts.json" if rec else "5000 per instance (no record)"},
+                   "ms_per_round_trip_min_max": {str(n): [round(min(acc[n]), 3), round(max(acc[n]), 3)]
+                                                 for n in SIZES},
+                   "value_spread_over_steps": [min(per_step_value), max(per_step_value)],
+                   "round_trips_source": ("tests/golden/cw_sweep_rts.json (round trips per instance recorded by "
+                                          "this project's FP32 solver under the same rule)") if rec else
+                                         "5000 per instance (no record)",
+                   "setup": "reference host code (ref_setup_cw2: src/cuOPO.cu:92-234 with its Sellmeier, "
+                            "linspace, fftshift, input_field_T), numpy-seeded noise"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "reference",
                          "sample": "reference crystal pass + cavity kernels with cuFFT on the GPU, driven by one host "
-                                   f"thread; {rts_per_step} round trips per grid size per step, scaled to the sweep"},
+                                   f"thread; {REF_RTS_PER_STEP} round trips per grid size per step, scaled to the "
+                                   "sweep"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line))
@@ -402,6 +466,9 @@ def run_cuopo(args):
                                                  "rts": rts[inv].tolist(), "flags": flags[inv].tolist(),
                                                  "ps": ps[inv].tolist()}))
 
+    # per-grid-size kernel timing (untimed for `value`): each grid size's instances of the sweep alone
+    per_size = time_per_size(cu, base, insts_o, peak, stream) if rank == 0 else None
+
     validation = None
     if not args.no_validate and rank == 0:
         validation = validate_fp64(cu, base, insts_o, h_init, ps, rts, flags)
@@ -411,10 +478,18 @@ def run_cuopo(args):
         # DRAM bytes per instance-point and launch from one ncu capture; a step is one launch per grid size
         rate = json.loads(TRAFFIC_RECORD.read_text()).get("dram_bytes_per_instance_point")
         traffic = rate * float(np.sum(nt_o)) if rate else None
+    dom = None
+    if per_size:
+        # the dominant kernel: the grid size with the largest share of the sweep's algorithmic work
+        work = {n: float(sum(r * flops_per_instance_rt(int(m), g) for r, m, g in zip(rts, nt_o, gdd_o) if m == n))
+                for n in set(nt_o.tolist())}
+        n_dom = max(work, key=work.get)
+        dom = dict(per_size[str(n_dom)], n_t=n_dom, share_of_sweep_flops=work[n_dom] / flops)
     if rank == 0:
         line = {
             "metric": METRIC,
             "value": done_all / (dev_ms * 1e-3),
+            "converged_solves_per_s": conv_all / (dev_ms * 1e-3),
             "unit": "solves/s",
             "n_gpus": world,
             "steps": K,
@@ -440,12 +515,20 @@ def run_cuopo(args):
             "slices_per_s": slices * world / (dev_ms * 1e-3),
             "point_slices_per_s": pt_slices * world / (dev_ms * 1e-3),
             "hbm_frac": (hbm_bytes / (dev_ms * 1e-3)) / (measured_hbm_gbs() * 1e9),
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
-                         "peak_source": "measured live: best of scalar and packed f32x2 FMA-chain probes (cuopo_probe_fp32_peak); "
-                                        "fields stay in shared memory, so neither HBM nor tensor cores bound it",
-                         "kernel": "ssfm_kernel (fused round trips, all grid sizes)"},
+            "roofline": ({"bound": "fp32", "achieved": dom["tflops"], "peak": peak, "unit": "TFLOP/s",
+                          "frac": dom["frac"], "traffic": dom["traffic_bytes"],
+                          "traffic_per": "launch (ncu-measured DRAM bytes per instance-point x instance-points)",
+                          "peak_source": "measured live: best of scalar and packed f32x2 FMA-chain probes "
+                                         "(cuopo_probe_fp32_peak); fields stay in shared memory, so neither HBM nor "
+                                         "tensor cores bound it",
+                          "kernel": f"ssfm_kernel, grid 2^{int(math.log2(dom['n_t']))} ({dom['kernel']}), "
+                                    f"{dom['share_of_sweep_flops']:.0%} of the sweep's algorithmic work; "
+                                    "CUDA events around its launch on the launching stream"} if dom else None),
+            "sweep_roofline": {"achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                               "frac": achieved / peak if peak else None, "traffic": traffic,
+                               "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
+                               "kernel": "ssfm_kernel (fused round trips, all grid sizes at once)"},
+            "per_size": per_size,
             "cpu_baseline": cpu,
             "e2e": {"value": done_all / (e2e_ms * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(total * 8 / K), "d2h_bytes_per_step": int((total * 8 + len(insts) * 16) / K)},
@@ -462,14 +545,57 @@ def run_cuopo(args):
     return 0
 
 
-def validate_fp64(cu, base, insts_o, h_init, ps, rts, flags, max_check=8):
-    """FP64 check of the output signal power: converged instances of the
-    smallest grid (non-trivial power) are re-run with an FP64 plan from the same
-    initial noise for the same number of round trips; reports the relative error
-    of the FP32 result's final signal power."""
+def time_per_size(cu, base, insts_o, peak, stream, n_rt: int = 20) -> dict:
+    """Each grid size's kernel alone: a batch of that size's sweep instances
+    runs n_rt round trips from noise (one launch) between CUDA events on the
+    launching stream; algorithmic TFLOP/s and fraction of the FP32 probe."""
     import torch
-    cand = [k for k, x in enumerate(insts_o) if flags[k] == 1 and ps[k] > 1e-20 and x["n_t"] == 4096]
-    idx = sorted(cand, key=lambda k: rts[k])[:max_check]
+    rate = None
+    if TRAFFIC_RECORD.exists():
+        rate = json.loads(TRAFFIC_RECORD.read_text()).get("dram_bytes_per_instance_point")
+    out = {}
+    for n in sorted(set(int(x["n_t"]) for x in insts_o)):
+        sub = [x for x in insts_o if x["n_t"] == n]
+        m, cl = cu.kernel_config(n)
+        with cu.Batch(base, sub) as b:
+            b.seed_noise(NOISE)
+            b.reset()
+            b.step(n_rt, n_rt, 0.0, 1)     # warm-up launch
+            b.reset()
+            b.wait(stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            b.step(n_rt, n_rt, 0.0, 1)
+            b.wait(stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            _, r, _ = b.results()
+        fl = float(sum(int(rr) * flops_per_instance_rt(n, x["gdd"]) for rr, x in zip(r, sub)))
+        tf = fl / (ms * 1e-3) / 1e12
+        out[str(n)] = {"kernel": f"{cl} x {m}-point CTA" + ("s" if cl > 1 else ""), "instances": len(sub),
+                       "round_trips": n_rt, "ms": round(ms, 3), "tflops": tf, "frac": tf / peak if peak else None,
+                       "point_slices_per_s": float(np.sum(r)) * n * N_Z / (ms * 1e-3),
+                       "traffic_bytes": rate * n * len(sub) if rate else None}
+    return out
+
+
+def validate_fp64(cu, base, insts_o, h_init, ps, rts, flags, per_class: int = 1):
+    """FP64 check of the output signal power, stratified: for every grid size,
+    `per_class` converged (non-trivial power) and `per_class` round-trip-limit
+    instances are re-run with an FP64 plan from the same initial noise for the
+    same number of round trips (all at once, one stream each); reports the
+    relative error of the FP32 final signal power per grid size and class."""
+    import torch
+    idx = []
+    for n in sorted(set(x["n_t"] for x in insts_o)):
+        for flag in (1, 2):
+            cand = [k for k, x in enumerate(insts_o) if x["n_t"] == n and flags[k] == flag and ps[k] > 1e-20]
+            cand.sort(key=lambda k: rts[k])
+            if cand:
+                # the median-round-trip member of the class (deterministic)
+                idx += [cand[len(cand) // 2]] if per_class == 1 else cand[:: max(1, len(cand) // per_class)][:per_class]
     if not idx:
         return {"checked": 0}
     offs = np.concatenate([[0], np.cumsum([x["n_t"] for x in insts_o])])
@@ -491,9 +617,13 @@ def validate_fp64(cu, base, insts_o, h_init, ps, rts, flags, max_check=8):
     for plan, _ in runs:
         plan.close()
     err = np.abs(ps[idx] - ps64) / np.abs(ps64)
-    return {"checked": len(idx), "rule": "FP64 plan, same initial noise, same round trips",
+    cases = [{"n_t": int(insts_o[k]["n_t"]), "class": "converged" if flags[k] == 1 else "rt_limit",
+              "rts": int(rts[k]), "rel_err_ps": float(e)} for k, e in zip(idx, err)]
+    return {"checked": len(idx), "rule": "FP64 plan, same initial noise, same round trips; per grid size the "
+                                         "median-round-trip converged and round-trip-limit instance",
             "max_rel_err_ps": float(np.max(err)), "median_rel_err_ps": float(np.median(err)),
-            "rts": rts[idx].tolist(), "seconds": round(time.perf_counter() - t0, 1)}
+            "frac_within_1e-5": float(np.mean(err <= 1e-5)), "cases": cases,
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def main():

@@ -1179,14 +1179,17 @@ extern "C" cuopo_status cuopo_kernel_config(int precision, int n_eqs, int n_t, i
 
 /*
  * cuopo_crystal_pass_noalloc: one crystal pass for callers that must not
- * allocate device memory -- code running while a CUDA graph is being
- * captured, processes whose device memory is owned by another allocator or
- * budget, or plugins loaded into such processes.  Its tables live in the
- * file-scope array below (every GPU that loads the library holds it until
- * exit); the host side builds them in a static host buffer and uploads them
- * with cudaMemcpyAsync.  The array is shared by every call, so calls that
- * overlap on the GPU (different streams, or different host threads without
- * ordering) race; calls ordered on one stream do not.
+ * allocate device memory -- processes whose device memory is owned by
+ * another allocator or budget, or plugins loaded into such processes.  Its
+ * tables live in the file-scope array below (every GPU that loads the
+ * library holds it until exit); the host side builds them in a static host
+ * buffer and uploads them with cudaMemcpyAsync (a pageable source: the
+ * copy has left the buffer when the call returns, so the next call may
+ * overwrite it).  The array is shared by every call, so calls that overlap
+ * on the GPU (different streams, or different host threads without
+ * ordering) race; calls ordered on one stream do not.  The array's device
+ * address is looked up once per device and kept, so the library must not
+ * be used across a cudaDeviceReset of that device.
  */
 #define CUOPO_NOALLOC_BYTES (384u * 1024u)
 #define CUOPO_NOALLOC_MAX_N 8192

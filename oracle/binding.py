@@ -26,11 +26,11 @@ _cache: dict[str, C.CDLL] = {}
 
 
 def build() -> None:
-    """Builds the C oracle (and oracle/_ref when the reference checkout exists)."""
+    """Builds the C oracle, and oracle/_ref through its recipe (build_ref.sh
+    finds the reference checkout, or CUOPO_REFERENCE_ROOT, and skips the
+    harness when the sources are absent)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "CC=gcc"], check=True)
-    ref_root = os.environ.get("CUOPO_REFERENCE_ROOT", "/root/reference")
-    if Path(ref_root, "src", "headers", "cwes2.cuh").exists():
-        subprocess.run([str(HERE / "build_ref.sh"), ref_root], check=True)
+    subprocess.run([str(HERE / "build_ref.sh")], check=True)
 
 
 def _load(path: Path) -> C.CDLL:
@@ -115,6 +115,17 @@ def solve(params, w, T, Ap, As, Ai, pump, n_rt: int, max_rt: int, tol: float, bi
 
 # ------------------------------------------------------- reference harness
 
+class RefParams(C.Structure):
+    """The harness's ref_params block (oracle/ref_harness.cu): the leading
+    fields of the solver parameter block, filled by the reference's own
+    set-up code (ref_setup_cw2) without the product library."""
+    _fields_ = ([(n, C.c_int) for n in ("n_eqs", "n_t", "n_z", "regime")] +
+                [(n, C.c_double) for n in ("vp", "vs", "vi", "b2p", "b2s", "b2i", "b3p", "b3s", "b3i", "dk", "kp",
+                                           "ks", "ki", "dz", "alpha_crp", "alpha_crs", "alpha_cri", "Rs", "Ri",
+                                           "delta", "gdd", "tod_s", "tod_i")] +
+                [("use_eom", C.c_int), ("eom_idler", C.c_int), ("mod_depth", C.c_double), ("fpm", C.c_double)])
+
+
 def ref_lib(crystal: str, size: int) -> C.CDLL:
     """The reference's own code (oracle/_ref) for crystal 'ppln'/'spplt' and grid size."""
     lib = _load(REF_DIR / f"libref_{crystal}_{size}.so")
@@ -137,10 +148,28 @@ def ref_lib(crystal: str, size: int) -> C.CDLL:
     lib.ref_input_field_gauss.restype = None
     lib.ref_input_field_gauss.argtypes = [_vp, C.c_float, _vp, C.c_float, C.c_int]
     lib.ref_size.restype = C.c_int
+    lib.ref_setup_cw2.restype = None
+    lib.ref_setup_cw2.argtypes = [C.c_double] * 7 + [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
     lib.ref_round_trips.restype = C.c_int
     lib.ref_round_trips.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
                                     C.c_int, C.c_int, _vp, C.c_double, _vp, _vp]
     return lib
+
+
+def ref_setup_cw2(size: int, lp_nm: float, lambda_um: float, n_thr: float, r_percent: float, delta_pi: float,
+                  gdd_ps2: float, lcr_mm: float, n_z: int):
+    """The reference's own 2-equation CW set-up (src/cuOPO.cu:92-234) for a
+    MgO:PPLN grid of `size` points: returns (RefParams, w, T, pump, t_rt, ap0)."""
+    lib = ref_lib("ppln", size)
+    p = RefParams()
+    w = np.zeros(size, np.float32)
+    T = np.zeros(size, np.float32)
+    pump = np.zeros(size, np.complex64)
+    t_rt = C.c_double()
+    ap0 = C.c_double()
+    lib.ref_setup_cw2(lp_nm, lambda_um, n_thr, r_percent, delta_pi, gdd_ps2, lcr_mm, n_z, C.byref(p),
+                      w.ctypes.data, T.ctypes.data, pump.ctypes.data, C.byref(t_rt), C.byref(ap0))
+    return p, w, T, pump, t_rt.value, ap0.value
 
 
 def ref_available(crystal: str, size: int) -> bool:

@@ -2,9 +2,12 @@
 # Builds the reference's own SSFM code (headers included in place from the
 # reference checkout) into oracle/_ref/libref_<crystal>_<size>.so.
 # Test infrastructure only.  Usage: oracle/build_ref.sh [reference_root]
+# The checkout is the argument, else $CUOPO_REFERENCE_ROOT, else the path
+# where this build environment mounts it; this recipe is the one place that
+# names it.  Without the sources (e.g. on a GPU box) it builds nothing.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${CUOPO_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-nvcc}"
 if [ ! -f "$REF/src/headers/cwes2.cuh" ]; then

@@ -27,6 +27,7 @@
 #include <iomanip>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <cmath>
 #include <chrono>
 #include <sys/time.h>
@@ -123,6 +124,62 @@ void ref_input_field_cw(float2 *A, float A0, int n) { input_field_T(A, A0, n); }
 void ref_input_field_gauss(float2 *A, float A0, float *T, float T0, int n)
 {
     input_field_T(A, A0, T, T0, n);
+}
+
+/*
+ * The 2-equation CW set-up of the reference's main program
+ * (src/cuOPO.cu:92-234), evaluated with the reference's own host functions
+ * (Sellmeier n/GV/GVD, findPhaseMatchingTemp, linspace, fftshift,
+ * input_field_T) in its float types: argv-level inputs in, the solver
+ * parameters, the grids T and w (n_t = SIZE points) and the CW pump out.
+ * Harness inputs beyond the reference's argv: gdd_ps2, the intracavity GDD
+ * in ps^2 (the reference takes a percentage of the crystal GDD,
+ * cuOPO.cu:141-142), and n_z.  Host only; needs no GPU.
+ */
+void ref_setup_cw2(double lp_nm, double Lambda_um, double Nth_in, double R_percent, double delta_pi,
+                   double gdd_ps2, double Lcr_mm, int n_z, ref_params *p, float *w_out, float *T_out,
+                   float2 *pump_out, double *t_rt_out, double *ap0_out)
+{
+    const real_t lp = lp_nm * 1e-3;                              /* cuOPO.cu:92-101 */
+    const real_t ls = 2 * lp;
+    const real_t Lambda = Lambda_um;
+    const real_t Temp = findPhaseMatchingTemp(lp, ls, Lambda, 10, 150);
+    const real_t Lcr = Lcr_mm * 1e3;
+    const real_t np = n(lp, Temp), vp = GV(lp, Temp), b2p = GVD(lp, Temp);  /* :103-114 */
+    const real_t kp = 2 * PI * dQ / (np * lp);
+    const real_t ns = n(ls, Temp), vs = GV(ls, Temp), b2s = GVD(ls, Temp);
+    const real_t ks = 2 * PI * dQ / (ns * ls);
+    const real_t dk = 2 * PI * (np / lp - 2 * ns / ls - 1 / Lambda);          /* :125 */
+    const real_t Lcav = 100e3;                                               /* :129-146 */
+    const real_t Rs = R_percent * 0.01;
+    const real_t alphas = 0.5 * ((1 - Rs) + alpha_crs * Lcr);
+    const real_t t_rt = (Lcav + Lcr * (ns - 1)) / C;
+    const real_t dz = Lcr / (real_t)(uint)n_z;                               /* :149-151 */
+    const real_t dF = 1 / t_rt;
+    linspace(T_out, SIZE, -0.5 * t_rt, 0.5 * t_rt);                          /* :170-189 */
+    real_t *Fq = (real_t *)malloc(sizeof(real_t) * SIZE);
+    linspace(Fq, SIZE, -0.5 * SIZE * dF, +0.5 * SIZE * dF);
+    fftshift(w_out, Fq, SIZE);
+    for (uint i = 0; i < SIZE; i++) w_out[i] = 2 * PI * w_out[i];
+    free(Fq);
+    const real_t waist = 55, spot = PI * waist * waist;                      /* :202-229 */
+    (void)spot;
+    const real_t Ith = EPS0 * C * np * powf((ns * ls * alphas / dQ / Lcr / PI), 2) / 8;
+    const real_t Inten = Nth_in * Ith;
+    const real_t Ap0 = sqrt(2 * Inten / (np * EPS0 * C));
+    input_field_T(pump_out, Ap0, SIZE);                                      /* :238-241 */
+
+    memset(p, 0, sizeof(*p));
+    p->n_eqs = 2;
+    p->n_t = (int)SIZE;
+    p->n_z = n_z;
+    p->regime = 0;
+    p->vp = vp; p->vs = vs; p->b2p = b2p; p->b2s = b2s;
+    p->dk = dk; p->kp = kp; p->ks = ks; p->dz = dz;
+    p->alpha_crp = alpha_crp; p->alpha_crs = alpha_crs; p->alpha_cri = alpha_cri;
+    p->Rs = Rs; p->Ri = 0.98f; p->delta = (real_t)delta_pi; p->gdd = (real_t)gdd_ps2;
+    *t_rt_out = t_rt;
+    *ap0_out = Ap0;
 }
 
 /* ---- the reference round-trip loop on the GPU ---- */

@@ -49,7 +49,8 @@ typedef ORACLE_REAL _Complex cplx;
 #define ORACLE_PI 3.14159265358979323846
 
 /* Parameter block.  Field order is part of the ctypes binding in
- * tests/oracle_lib.py; keep the two in step. */
+ * oracle/binding.py (which passes the library's cuopo_params struct, whose
+ * leading fields are these); keep them in step. */
 typedef struct {
     int n_eqs;          /* 2 or 3 coupled-wave equations (THREE_EQS) */
     int n_t;            /* grid points per round trip (SIZE, a power of 2) */

@@ -112,3 +112,26 @@ def test_derived_c1_values():
     assert abs(info.temp_c - 26.859371) < 1e-5
     assert p.dz == 50.0 and p.n_t == 8192
     assert 0.09 < p.ap0 < 0.1
+
+
+@pytest.mark.parametrize("n_t", [4096, 8192, 16384, 32768])
+@pytest.mark.parametrize("n_thr,r_percent,delta,gdd_fs2", [(4.0, 98.0, 0.0, 0.0), (1.37, 90.4, -0.61, 321.5),
+                                                          (5.83, 98.9, 0.97, -488.0)])
+def test_reference_cw_setup_matches_product(n_t, n_thr, r_percent, delta, gdd_fs2):
+    """The harness's restatement of the reference's 2-equation CW set-up
+    (src/cuOPO.cu:92-234, used by the benchmark's reference arm without the
+    product library) equals the product's cuopo_derive_params, grids and CW
+    pump bit for bit."""
+    if not ob.ref_available("ppln", n_t):
+        pytest.skip("reference harness not built for this grid")
+    from cuopo_b200 import sweep
+    p, _ = cu.derive_params(sweep.cw_base_inputs(n_t=n_t, n_z=100, n_thr=n_thr, r_percent=r_percent))
+    T, w = cu.make_grids(n_t, p.t_rt)
+    pump = cu.pump_cw(n_t, p.ap0)
+    rp, rw, rT, rpump, t_rt, ap0 = ob.ref_setup_cw2(n_t, 532.0, 6.970206862971646, n_thr, r_percent, delta,
+                                                    gdd_fs2 * 1e-6, 5.0, 100)
+    for name in ("vp", "vs", "b2p", "b2s", "dk", "kp", "ks", "dz", "alpha_crp", "alpha_crs", "Rs", "Ri"):
+        assert getattr(rp, name) == getattr(p, name), name
+    assert rp.delta == f32(delta) and rp.gdd == f32(gdd_fs2 * 1e-6)
+    assert (t_rt, ap0) == (p.t_rt, p.ap0)
+    assert np.array_equal(rw, w) and np.array_equal(rT, T) and np.array_equal(rpump, pump)
