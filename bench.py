@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--autotune", action="store_true",
                     help="time each grid size's kernel configurations first (cuopo_autotune); default: the built-in "
                          "order, measured on batches of every grid size running together")
+    ap.add_argument("--warm-count", type=int, default=296,
+                    help="held-out instances (2^13 points) of the learned warm-start comparison (0: skip)")
     ap.add_argument("--split", action="store_true",
                     help="N > 1: split one sweep of --count instances over the ranks (strong scaling) instead of "
                          "giving every rank its own sweep (weak scaling, the default)")
@@ -472,6 +474,7 @@ def run_cuopo(args):
     validation = None
     if not args.no_validate and rank == 0:
         validation = validate_fp64(cu, base, insts_o, h_init, ps, rts, flags)
+    warm_leg = warm_start_leg(args) if rank == 0 and args.warm_count > 0 else None
 
     traffic = None
     if TRAFFIC_RECORD.exists():
@@ -535,6 +538,7 @@ def run_cuopo(args):
             "gpu_launches": K * len(set(nt_o.tolist())) + 0,
             "clocks": clk,
             "validation_fp64": validation,
+            "warm_start": warm_leg,
         }
         print(json.dumps(line))
     batch.close()
@@ -578,6 +582,63 @@ def time_per_size(cu, base, insts_o, peak, stream, n_rt: int = 20) -> dict:
                        "round_trips": n_rt, "ms": round(ms, 3), "tflops": tf, "frac": tf / peak if peak else None,
                        "point_slices_per_s": float(np.sum(r)) * n * N_Z / (ms * 1e-3),
                        "traffic_bytes": rate * n * len(sub) if rate else None}
+    return out
+
+
+def measured_bf16_tflops() -> float | None:
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
+def warm_start_leg(args, seed: int = 7) -> dict:
+    """The learned warm start (cuopo_b200/data/warmstart_mlp.npz): held-out
+    instances of the sweep's distribution at 2^13 points solved from noise
+    and from the network's prediction by the same batched solver and rule
+    (warmstart.evaluate); plus the network's tensor-core kernels timed alone:
+    one training step (forward, backward, Adam; CUDA graph) at batch 4096 and
+    inference, against the measured BF16 peak."""
+    import torch
+    from cuopo_b200 import warmstart as ws
+    if not ws.MODEL_PATH.exists():
+        return {"unavailable": f"no trained model at {ws.MODEL_PATH.relative_to(ROOT)}"}
+    model = ws.WarmStartModel.load()
+    out = ws.evaluate(model, args.warm_count, seed, n_t=8192, max_rt=args.max_rt, tol=TOL)
+    out["model"] = model.meta
+    # the network's kernels alone
+    mlp = ws.MLP(max_batch=4096, seed=1)
+    x = torch.rand(4096, ws.N_FEATURES, device="cuda") * 2 - 1
+    t = torch.randn(4096, 2 * ws.N_MODES, device="cuda")
+    for _ in range(5):
+        mlp.train_step(x, t, 1e-4)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    n = 50
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(n):
+        mlp.train_step(x, t, 1e-4)
+    ev[1].record()
+    for _ in range(n):
+        mlp.forward(x)
+    ev[2].record()
+    torch.cuda.synchronize()
+    mlp.status()
+    mlp.close()
+    train_ms = ev[0].elapsed_time(ev[1]) / n
+    fwd_ms = ev[1].elapsed_time(ev[2]) / n
+    w, d, k0 = ws.WIDTH, ws.DEPTH, 64
+    fwd_flops = 2.0 * 4096 * (k0 * w + (d - 1) * w * w + w * 2 * ws.N_MODES)
+    train_flops = 3.0 * fwd_flops - 2.0 * 4096 * k0 * w      # forward, dW of every layer, dX of all but the first
+    peak = measured_bf16_tflops()
+    out["tensor_cores"] = {
+        "train_step_us": 1e3 * train_ms, "train_tflops": train_flops / (train_ms * 1e-3) / 1e12,
+        "forward_us": 1e3 * fwd_ms, "forward_tflops": fwd_flops / (fwd_ms * 1e-3) / 1e12,
+        "bf16_peak_tflops": peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)",
+        "train_frac": (train_flops / (train_ms * 1e-3) / 1e12) / peak if peak else None,
+        "note": "batch 4096, 4 -> 512 x 4 (GELU) -> 512; layer 0 padded to K = 64; the training step is one "
+                "CUDA graph (14 tcgen05 GEMM launches, loss and Adam) after an input-packing kernel"}
+    model.close()
     return out
 
 

@@ -15,7 +15,7 @@ LIB_PATH = HERE / "libcuopo_b200.so"
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ENONFINITE, EUNSUPPORTED, EIO = range(8)
 PPLN, SPPLT = 0, 1
 CW, NS = 0, 1
-F32, F64 = 0, 1
+F32, F64, F32_PHASE32 = 0, 1, 2
 
 _STATUS_NAMES = {0: "CUOPO_OK", 1: "CUOPO_EINVAL", 2: "CUOPO_ENOMEM", 3: "CUOPO_ECUDA", 4: "CUOPO_ETIMEOUT",
                  5: "CUOPO_ENONFINITE", 6: "CUOPO_EUNSUPPORTED", 7: "CUOPO_EIO"}
@@ -121,6 +121,18 @@ SIGNATURES = {
     "cuopo_autotune_reset": (_i, []),
     "cuopo_kernel_select": (_i, [_i, _i, _i, _i, _i]),
     "cuopo_kernel_config": (_i, [_i, _i, _i, C.POINTER(_i), C.POINTER(_i)]),
+    "cuopo_mlp_create": (_i, [C.POINTER(_vp), _i, _i, _i, _i, _i, C.c_uint64]),
+    "cuopo_mlp_destroy": (_i, [_vp]),
+    "cuopo_mlp_param_count": (_i, [_vp, C.POINTER(C.c_long)]),
+    "cuopo_mlp_set_params": (_i, [_vp, _vp]),
+    "cuopo_mlp_get_params": (_i, [_vp, _vp]),
+    "cuopo_mlp_forward": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "cuopo_mlp_gradients": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp]),
+    "cuopo_mlp_train_step": (_i, [_vp, _vp, _vp, _i, C.c_float, _vp, _vp]),
+    "cuopo_mlp_status": (_i, [_vp]),
+    "cuopo_gemm_bf16": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
+    "cuopo_fields_from_modes": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
+    "cuopo_modes_from_spectrum": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

@@ -170,7 +170,7 @@ class Plan:
 
     def _check_fields(self, *fields):
         import torch
-        want = torch.complex64 if self.precision == F32 else torch.complex128
+        want = torch.complex128 if self.precision == F64 else torch.complex64
         for f in fields:
             if f is None:
                 continue

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CC_FLAGS = ["-O2", "-fPIC", "-std=c11", "-Wall", "-Wextra", "-fvisibility=hidden", "-I" + str(INCLUDE),
             "-I" + str(CSRC)]
 
-CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu", "probe.cu"]
+CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu", "probe.cu", "mlp.cu"]
 C_SOURCES = ["params.c", "dat_io.c"]
 BIN = HERE / "bin"
 CLI = BIN / "cuopo"

@@ -21,7 +21,8 @@ using namespace cuopo;
 
 struct cuopo_plan {
     cuopo_params p;
-    int precision;
+    int precision;    /* CUOPO_F32 or CUOPO_F64: the field type and kernel */
+    int phase32;      /* CUOPO_F32_PHASE32 plans: phase factors in FP32 */
     int F;            /* number of fields */
     int N;            /* grid points */
     int threads;      /* CTA size */
@@ -229,11 +230,28 @@ static void stage_times(const cuopo_params &p, int s_count, std::vector<double> 
     }
 }
 
+/* sin and cos of a phase: in FP64, or (p32) in FP32 after reducing the
+ * argument to [-pi, pi] in FP64 -- the CUOPO_F32_PHASE32 variant, the
+ * cheapest way a float build forms e^{i ph} without losing a large argument
+ * (the reference uses FP32 cos/sin of a float argument,
+ * src/headers/operators.cuh:120-126). */
+static void phase_sc(double ph, bool p32, double &sn, double &cs)
+{
+    if (p32) {
+        const float r = (float)std::remainder(ph, 2.0 * M_PI);
+        sn = (double)sinf(r);
+        cs = (double)cosf(r);
+    } else {
+        sn = std::sin(ph);
+        cs = std::cos(ph);
+    }
+}
+
 template <typename R>
 static std::vector<unsigned char> build_tables(const cuopo_params &p, const float *w, const float *T, int CL,
                                                std::vector<unsigned char> &rk_out,
                                                std::vector<unsigned char> &eom_out,
-                                               std::vector<unsigned char> &twn_out, double &h6)
+                                               std::vector<unsigned char> &twn_out, double &h6, bool p32 = false)
 {
     using C = cpx<R>;
     const int N = p.n_t;
@@ -269,8 +287,10 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
              * ulp of att, which would compound over thousands of round trips. */
             const int k2 = k % CL, k1 = k / CL;
             const double a = att * (double)N;
-            const double dre = (ph == 0.0) ? a - 1.0 : a * std::cos(ph) - 1.0;
-            D[(size_t)f * N + (size_t)k2 * M + k1] = mk<C>((R)dre, (R)(a * std::sin(ph)));
+            double sn, cs;
+            phase_sc(ph, p32, sn, cs);
+            const double dre = (ph == 0.0) ? a - 1.0 : a * cs - 1.0;
+            D[(size_t)f * N + (size_t)k2 * M + k1] = mk<C>((R)dre, (R)(a * sn));
         }
     }
     /* cross-stage twiddles W_N^q = exp(2 pi i q / N) as a quarter turn
@@ -300,7 +320,8 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
             /* dAdz, cwes2.cuh:37-38: i kp e^{+i dk z}, i ks e^{-i dk z} */
             for (int j = 0; j < 3; j++) {
                 const double ph = p.dk * zs[3 * s + j];
-                const double c = std::cos(ph), sn = std::sin(ph);
+                double c, sn;
+                phase_sc(ph, p32, sn, c);
                 co[s * 6 + 2 * j + 0] = mk<C>((R)(-p.kp * sn), (R)(p.kp * c));
                 co[s * 6 + 2 * j + 1] = mk<C>((R)(p.ks * sn), (R)(p.ks * c));
             }
@@ -310,9 +331,10 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
             double er = 0, ei = 0;
             const double wgt[3] = {1.0, 4.0, 1.0};
             for (int j = 0; j < 3; j++) {
-                const double ph = p.dk * zs[3 * s + j];
-                er += wgt[j] * std::cos(ph);
-                ei += wgt[j] * std::sin(ph);
+                double c, sn;
+                phase_sc(p.dk * zs[3 * s + j], p32, sn, c);
+                er += wgt[j] * c;
+                ei += wgt[j] * sn;
             }
             /* pump: E- = conj(E+) */
             const double kap[3] = {p.kp, p.ks, p.ki};
@@ -329,8 +351,10 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
         eom_out.resize(sizeof(C) * (size_t)N);
         C *E = reinterpret_cast<C *>(eom_out.data());
         for (int k = 0; k < N; k++) {
-            const double ph = p.mod_depth * std::sin(2.0 * M_PI * p.fpm * (double)T[k]);
-            E[k] = mk<C>((R)std::cos(ph), (R)std::sin(ph));
+            double s1, c1, sn, cs;
+            phase_sc(2.0 * M_PI * p.fpm * (double)T[k], p32, s1, c1);
+            phase_sc(p.mod_depth * s1, p32, sn, cs);
+            E[k] = mk<C>((R)cs, (R)sn);
         }
     }
     return disp;
@@ -344,8 +368,10 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
     if (p->n_eqs != 2 && p->n_eqs != 3) return cuopo_fail(CUOPO_EINVAL, "n_eqs must be 2 or 3");
     if (!is_pow2i(p->n_t)) return cuopo_fail(CUOPO_EINVAL, "n_t must be a power of 2");
     if (p->n_z < 1) return cuopo_fail(CUOPO_EINVAL, "n_z must be >= 1");
-    if (precision != CUOPO_F32 && precision != CUOPO_F64)
-        return cuopo_fail(CUOPO_EINVAL, "precision must be CUOPO_F32 or CUOPO_F64");
+    if (precision != CUOPO_F32 && precision != CUOPO_F64 && precision != CUOPO_F32_PHASE32)
+        return cuopo_fail(CUOPO_EINVAL, "precision must be CUOPO_F32, CUOPO_F64 or CUOPO_F32_PHASE32");
+    const bool phase32 = precision == CUOPO_F32_PHASE32;
+    if (phase32) precision = CUOPO_F32;
     const KernelEntry *k = find_kernel(precision, p->n_eqs, p->n_t);
     if (!k) return cuopo_fail(CUOPO_EUNSUPPORTED, "no kernel built for this (precision, n_eqs, n_t)");
 
@@ -362,7 +388,7 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
     std::vector<unsigned char> disp, rk, eom, twn;
     double h6 = 0;
     const int CL = k->CL;
-    if (precision == CUOPO_F32) disp = build_tables<float>(*p, w.data(), T.data(), CL, rk, eom, twn, h6);
+    if (precision == CUOPO_F32) disp = build_tables<float>(*p, w.data(), T.data(), CL, rk, eom, twn, h6, phase32);
     else disp = build_tables<double>(*p, w.data(), T.data(), CL, rk, eom, twn, h6);
     /* frequency grid in the same per-CTA order as the dispersion table */
     std::vector<float> wp((size_t)p->n_t);
@@ -372,6 +398,7 @@ extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *
     if (!pl) return cuopo_fail(CUOPO_ENOMEM, "plan_create: out of host memory");
     pl->p = *p;
     pl->precision = precision;
+    pl->phase32 = phase32;
     pl->F = p->n_eqs;
     pl->N = p->n_t;
     pl->threads = k->M / 16;
@@ -482,15 +509,16 @@ static LaunchArgs base_args(const cuopo_plan *pl)
     return a;
 }
 
-static void cavity_factors(const cuopo_params &p, Instance &I)
+static void cavity_factors(const cuopo_params &p, Instance &I, bool p32 = false)
 {
     /* AddPhase: sqrt(R) * exp(i pi delta), functions.cuh:145 */
-    const double ph = M_PI * p.delta;
+    double sn, cs;
+    phase_sc(M_PI * p.delta, p32, sn, cs);
     const double rs = std::sqrt(p.Rs), ri = std::sqrt(p.Ri);
-    I.phase_s[0] = rs * std::cos(ph);
-    I.phase_s[1] = rs * std::sin(ph);
-    I.phase_i[0] = ri * std::cos(ph);
-    I.phase_i[1] = ri * std::sin(ph);
+    I.phase_s[0] = rs * cs;
+    I.phase_s[1] = rs * sn;
+    I.phase_i[0] = ri * cs;
+    I.phase_i[1] = ri * sn;
     I.gdd = p.gdd;
     I.tod_s = p.tod_s;
     I.tod_i = p.tod_i;
@@ -551,7 +579,7 @@ extern "C" cuopo_status cuopo_round_trips(cuopo_plan *pl, void *Ap, void *As, vo
     I.ps_hist = ps_hist;
     I.tol = tol;
     I.rt_done = rt_done_dev;
-    cavity_factors(pl->p, I);
+    cavity_factors(pl->p, I, pl->phase32);
     return launch(pl, a, 1, stream);
 }
 

@@ -40,7 +40,14 @@ typedef enum {
 
 enum { CUOPO_PPLN = 0, CUOPO_SPPLT = 1 };   /* -DPPLN / -DSPPLT */
 enum { CUOPO_CW = 0, CUOPO_NS = 1 };        /* -DCW_OPO / -DNS_OPO */
-enum { CUOPO_F32 = 0, CUOPO_F64 = 1 };      /* field precision */
+/* Field precision.  CUOPO_F32: complex64 fields, every phase factor formed
+ * in FP64 and rounded once; CUOPO_F64: complex128 fields and FP64
+ * arithmetic; CUOPO_F32_PHASE32 (plans only): complex64 fields with the
+ * phase factors (dispersion, RK4 stage phases, modulator, AddPhase) formed
+ * by FP32 sin/cos after FP64 reduction of the argument to [-pi, pi] -- the
+ * third variant of the precision study (the GDD/TOD factor formed inside
+ * the kernel stays FP64). */
+enum { CUOPO_F32 = 0, CUOPO_F64 = 1, CUOPO_F32_PHASE32 = 2 };
 
 /*
  * Solver parameters: the arguments of EvolutionInCrystal
@@ -327,21 +334,96 @@ cuopo_status cuopo_kernel_config(int precision, int n_eqs, int n_t, int *points_
 
 /*
  * One crystal pass that allocates no device memory, for callers that cannot
- * call cudaMalloc: code running while a CUDA graph is being captured, or a
- * plugin in a process whose device memory belongs to another allocator.  It
- * has no counterpart in the reference (whose caller allocates every buffer,
- * src/cuOPO.cu:384-442).  Same computation as cuopo_crystal_pass on an FP32
- * plan built from (p, w_host); fields are float pairs (device).  Its tables
- * are written into a fixed 384 KiB device array inside this library (held
- * by every GPU that loads it until exit), so n_t must be a power of 2 in
- * [512, 8192] and n_z in [1, 1024]; larger sizes return CUOPO_EINVAL.  The
- * first call on a device looks up that array's address (make it before any
- * stream capture); the array is shared by all calls, so calls that overlap
- * on the GPU race -- order them on one stream.  w_host: the n_t angular
- * frequencies, or NULL to build them from p->t_rt.
+ * call cudaMalloc: a plugin in a process whose device memory belongs to
+ * another allocator (a framework's caching allocator or a fixed memory
+ * budget, where a cudaMalloc behind its back can fail or fragment its
+ * pool).  It has no counterpart in the reference (whose caller allocates
+ * every buffer, src/cuOPO.cu:384-442).  Same computation as
+ * cuopo_crystal_pass on an FP32 plan built from (p, w_host); fields are
+ * float pairs (device).  Its tables are built on the host and copied with
+ * cudaMemcpyAsync from a static host buffer into a fixed 384 KiB device
+ * array inside this library (held by every GPU that loads it until exit),
+ * so n_t must be a power of 2 in [512, 8192] and n_z in [1, 1024]; larger
+ * sizes return CUOPO_EINVAL.  What is tested: calls ordered on one stream,
+ * each matching cuopo_crystal_pass.  The first call on a device looks up
+ * that array's address and keeps it for the life of the process (so the
+ * library must not be used across a cudaDeviceReset of that device).  The
+ * array is shared by all calls and keeps the last call's tables, so calls
+ * that overlap on the GPU race -- order them on one stream.  The pass does
+ * not report non-finite fields (there is no status to read back; check the
+ * fields).  w_host: the n_t angular frequencies, or NULL to build them from
+ * p->t_rt.
  */
 cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const float *w_host, void *Ap, void *As,
                                         void *Ai, void *stream);
+
+/* ---------------------------------------------- learned warm start (MLP) */
+
+/*
+ * A multilayer perceptron n_in -> width (GELU) x depth -> n_out that maps a
+ * cavity's parameters to the low-order Fourier modes of its steady-state
+ * signal; the solver starts from its prediction instead of noise.  No
+ * counterpart in the reference, which always starts from noise
+ * (src/headers/functions.cuh:58-71).  Weights and activations are BF16 on
+ * the tensor cores (tcgen05) with FP32 accumulation; FP32 master weights,
+ * Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the mean squared error over
+ * all outputs.  Limits: 1 <= n_in <= 64, width and n_out multiples of 128
+ * (n_out <= 1024), 1 <= depth <= 10.  Device buffers are sized for
+ * max_batch rows (rounded up to 128).  Weights start uniform in
+ * +-sqrt(6 / fan_in) from `seed`, biases at zero.
+ */
+typedef struct cuopo_mlp cuopo_mlp;
+
+cuopo_status cuopo_mlp_create(cuopo_mlp **mlp, int n_in, int width, int depth, int n_out, int max_batch,
+                              uint64_t seed);
+cuopo_status cuopo_mlp_destroy(cuopo_mlp *mlp);
+/* Number of parameters in the flat layout below. */
+cuopo_status cuopo_mlp_param_count(const cuopo_mlp *mlp, long *n);
+/* Flat FP32 host arrays, per layer l = 0..depth: W_l [n_out_l][n_in_l]
+ * (row-major) then b_l [n_out_l].  set_params also clears the Adam state.
+ * Synchronous. */
+cuopo_status cuopo_mlp_set_params(cuopo_mlp *mlp, const float *host);
+cuopo_status cuopo_mlp_get_params(cuopo_mlp *mlp, float *host);
+/* Inference: x [batch][n_in] -> y [batch][n_out], FP32 device arrays. */
+cuopo_status cuopo_mlp_forward(cuopo_mlp *mlp, const float *x, float *y, int batch, void *stream);
+/* Loss (mean squared error over batch x n_out) and its gradient with
+ * respect to every parameter (host array, flat layout) without an update.
+ * x, t: device.  Synchronous. */
+cuopo_status cuopo_mlp_gradients(cuopo_mlp *mlp, const float *x, const float *t, int batch, float *grad_host,
+                                 float *loss_host, void *stream);
+/* One Adam step on the batch (x, t device); the first call for a batch
+ * size and stream captures forward, loss, backward and update in a CUDA
+ * graph that later calls replay.  loss: device float of the batch's loss
+ * before the update, or NULL.  Asynchronous. */
+cuopo_status cuopo_mlp_train_step(cuopo_mlp *mlp, const float *x, const float *t, int batch, float lr, float *loss,
+                                  void *stream);
+/* Waits for the device and reports CUOPO_ETIMEOUT if a GEMM's bounded wait
+ * gave up since the last check. */
+cuopo_status cuopo_mlp_status(cuopo_mlp *mlp);
+/* The tensor-core GEMM alone: C[M][N] (FP32) = A[M][K] B[N][K]^T with A and
+ * B row-major BF16 on the device; M a multiple of 128, N of 64, K of 64;
+ * K split over `split` CTAs per tile (dividing K/64; C accumulated with
+ * atomics when split > 1).  err_dev: device int that gets bit 0 if a
+ * bounded wait (about 1 s) gave up, or NULL.  flags bit 0 is a test hook:
+ * the tile's completion barrier is never signalled, so every CTA's wait
+ * runs out, sets bit 0 and the CTA returns without storing (C is left
+ * as it was). */
+cuopo_status cuopo_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int split, int flags,
+                             int *err_dev, void *stream);
+
+/* Warm-start fields: `modes` holds per instance n_modes complex values
+ * (re, im pairs) of the Fourier modes q = -n_modes/2 .. n_modes/2-1 (cycles
+ * per round trip).  fields_from_modes writes each instance's n_t-point
+ * time-domain field scale * sum_q c_q exp(+2 pi i q n / n_t) (the same
+ * continuous field on any grid; n_modes a multiple of 16, <= 1024);
+ * modes_from_spectrum reads the modes back from the cuopo_fft_c2c sign -1
+ * transform of a field (divided by n_t * scale) with the sign that makes
+ * the largest mode's real part >= 0 (the 2-wave equations are invariant
+ * under As -> -As).  Device arrays; fields are float pairs. */
+cuopo_status cuopo_fields_from_modes(const float *modes, int count, int n_modes, int n_t, double scale, void *fields,
+                                     void *stream);
+cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, int n_t, int n_modes, double scale, float *modes,
+                                       void *stream);
 
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 3
  * launches each of a scalar and a packed FP32x2 FMA-chain kernel over every
