@@ -133,6 +133,7 @@ SIGNATURES = {
     "cuopo_gemm_bf16": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
     "cuopo_fields_from_modes": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
     "cuopo_modes_from_spectrum": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
+    "cuopo_fields_from_bands": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp]),
     "cuopo_sync": (_i, [_vp]),
     "cuopo_last_error": (C.c_char_p, []),
     "cuopo_version": (C.c_char_p, []),

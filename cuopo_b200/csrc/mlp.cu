@@ -11,11 +11,13 @@
  * 128 x BN output tile per CTA, the K loop pipelined through STAGES
  * shared-memory buffers (one TMA producer thread, one MMA issuer thread,
  * mbarriers in between), the accumulator in tensor memory, and a fused
- * epilogue run by all four warps (TMEM lanes = tile rows):
- *   forward    z = A W^T + b, h = GELU(z): stores z, h and h^T (BF16);
+ * epilogue run by 16 warps (TMEM lanes = tile rows, 4 lane quadrants x up
+ * to 4 chunks of 32 columns):
+ *   forward    z = A W^T + b, h = GELU(z): stores GELU'(z), h and h^T (BF16);
  *   output     y = A W^T + b (FP32);
- *   dX         g_prev = (g W) * GELU'(z_prev): stores g_prev, g_prev^T and
- *              adds the column sums of g_prev into the bias gradient;
+ *   dX         g_prev = (g W) * GELU'(z_prev) (the stored derivative):
+ *              stores g_prev, g_prev^T and adds the column sums of g_prev
+ *              into the bias gradient;
  *   dW         grad_W += g^T act over a K slice (split over the batch,
  *              FP32 atomics).
  * Keeping every activation and gradient in both layouts (row-major and
@@ -47,7 +49,7 @@ typedef __nv_bfloat16 bf16;
 constexpr int BM = 128;      /* tile rows = TMEM lanes */
 constexpr int BK = 64;       /* K per stage: 64 BF16 = one 128-byte swizzle row */
 constexpr int STAGES = 4;
-constexpr int NTHREADS = 128;
+constexpr int NTHREADS = 512;   /* 16 warps: 4 TMEM lane quadrants x up to 4 column chunks */
 constexpr unsigned long long WAIT_NS = 1000000000ull;
 
 /* ------------------------------------------------------------ PTX helpers */
@@ -182,10 +184,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 
-__device__ __forceinline__ float gelu_grad(float x)
-{
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
-}
 
 /* ------------------------------------------------------------ epilogue */
 
@@ -193,9 +191,9 @@ struct Epi {
     int ldo;              /* row stride of the row-major outputs (= N of the GEMM) */
     int ldt;              /* row stride of the transposed output */
     const float *bias;    /* [N] added first, or NULL */
-    int act;              /* 0 none, 1 GELU, 2 multiply by GELU'(z_in) */
-    const bf16 *z_in;     /* [M][ldo] for act 2 */
-    bf16 *z_out;          /* pre-activation [M][ldo], or NULL */
+    int act;              /* 0 none, 1 GELU, 2 multiply by gp_in */
+    const bf16 *gp_in;    /* GELU'(z) [M][ldo] for act 2 */
+    bf16 *gp_out;         /* act 1: GELU'(z) of the pre-activation z [M][ldo], or NULL */
     bf16 *out_bf;         /* [M][ldo], or NULL */
     bf16 *out_bfT;        /* [N][ldt], or NULL */
     float *out_f;         /* [M][ldo], or NULL */
@@ -246,15 +244,27 @@ __device__ __forceinline__ void epilogue32(const Epi &ep, int row, int col, floa
         for (int j = 0; j < 32; j++) v[j] += __ldg(ep.bias + col + j);
     }
     const size_t o = (size_t)row * ep.ldo + col;
-    if (ep.z_out && store) store_bf16x32(ep.z_out + o, v);
     if (ep.act == 1) {
+        if (ep.gp_out) {
+            /* GELU and its derivative from one erf: h = z Phi(z), h' = Phi(z) + z phi(z) */
+            float gp[32];
 #pragma unroll
-        for (int j = 0; j < 32; j++) v[j] = gelu(v[j]);
+            for (int j = 0; j < 32; j++) {
+                const float z = v[j];
+                const float ph = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+                gp[j] = ph + z * 0.39894228040143268f * expf(-0.5f * z * z);
+                v[j] = z * ph;
+            }
+            if (store) store_bf16x32(ep.gp_out + o, gp);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) v[j] = gelu(v[j]);
+        }
     } else if (ep.act == 2) {
-        float z[32];
-        load_bf16x32(ep.z_in + o, z);
+        float gp[32];
+        load_bf16x32(ep.gp_in + o, gp);
 #pragma unroll
-        for (int j = 0; j < 32; j++) v[j] *= gelu_grad(z[j]);
+        for (int j = 0; j < 32; j++) v[j] *= gp[j];
     }
     if (ep.out_f && store) {
         float4 *d = reinterpret_cast<float4 *>(ep.out_f + o);
@@ -299,15 +309,16 @@ constexpr size_t gemm_smem_bytes()
 
 /*
  * C tile (blockIdx.x, blockIdx.y) over the K slice blockIdx.z * kb_per ..
- * (+kb_per) blocks of 64.  128 threads: thread 0 issues the TMA loads,
- * thread 32 the MMAs; all four warps run the epilogue.
+ * (+kb_per) blocks of 64.  512 threads: thread 0 issues the TMA loads,
+ * thread 32 the MMAs; after the last MMA every warp runs the epilogue of
+ * one 32 x 32 block of the tile.
  */
 template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const Epi ep,
                    int kb_per)
 {
-    static_assert(BN == 64 || BN == 128 || BN == 256, "tile width");
+    static_assert(BN == 64 || BN == 128, "tile width: one 32-column chunk per warp and quadrant");
     extern __shared__ uint8_t smem_dyn[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_dyn + 1023) & ~(uintptr_t)1023);
     constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
@@ -334,12 +345,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *slot;
 
-    bool ok = true;
+    __shared__ int s_err;
+    if (threadIdx.x == 0) s_err = 0;
+    __syncthreads();
     if (threadIdx.x == 0) {
         for (int kb = 0; kb < kb_per; kb++) {
             const int s = kb % STAGES;
             if (kb >= STAGES && !mbar_wait(empty + s, ((kb / STAGES) & 1) ^ 1)) {
-                ok = false;
+                atomicOr(&s_err, 1);
                 break;
             }
             mbar_expect_tx(full + s, A_BYTES + B_BYTES);
@@ -351,7 +364,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int kb = 0; kb < kb_per; kb++) {
             const int s = kb % STAGES;
             if (!mbar_wait(full + s, (kb / STAGES) & 1)) {
-                ok = false;
+                atomicOr(&s_err, 1);
                 break;
             }
             tc_fence_after();
@@ -364,17 +377,20 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!ep.hold_done) umma_commit(done);   /* arrives when every MMA above has completed */
     }
     __syncwarp();
-    if (!mbar_wait(done, 0)) ok = false;
+    if (!mbar_wait(done, 0)) atomicOr(&s_err, 1);
+    /* every role loop and every wait above has ended (all are bounded) */
+    __syncthreads();
     tc_fence_after();
-    const bool store = !__any_sync(0xffffffffu, !ok);
-    const int row = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c = 0; c < BN; c += 32) {
+    const bool store = s_err == 0;
+    /* warp w reads TMEM lane quadrant w % 4 (the lanes it may access) and
+     * column chunk w / 4 of 32 */
+    const int quad = warp & 3, chunk = warp >> 2;
+    if (chunk < BN / 32) {
         float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-        epilogue32(ep, row, n0 + c, v, lane, store);
+        tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(chunk * 32), v);
+        epilogue32(ep, m0 + quad * 32 + lane, n0 + chunk * 32, v, lane, store);
     }
-    if (!store && lane == 0 && ep.err) atomicOr(ep.err, 1);
+    if (!store && threadIdx.x == 0 && ep.err) atomicOr(ep.err, 1);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, BN);
@@ -625,7 +641,8 @@ struct cuopo_mlp {
     int *err, *step;
     bf16 *xin, *xinT;
     std::vector<bf16 *> w_bf, wT_bf;                  /* per layer [N][Kp], [Kp][N] */
-    std::vector<bf16 *> z, h, hT, g, gT;              /* per hidden layer [rows][width] / [width][rows] */
+    std::vector<bf16 *> gp, h, hT, g, gT;             /* per hidden layer [rows][width] / [width][rows];
+                                                         gp = GELU'(z) */
     bf16 *g_out, *g_outT;
     std::vector<CUtensorMap> mA_fwd, mB_fwd, mA_dW, mB_dW, mA_dX, mB_dX;
     std::vector<void *> allocs;
@@ -668,7 +685,7 @@ cuopo_status forward(cuopo_mlp *m, int rows_used, bool train, cudaStream_t st)
             ep.act = 1;
             ep.out_bf = m->h[l];
             if (train) {
-                ep.z_out = m->z[l];
+                ep.gp_out = m->gp[l];
                 ep.out_bfT = m->hT[l];
             }
         } else {
@@ -709,7 +726,7 @@ cuopo_status backward(cuopo_mlp *m, int batch, int rows_used, cudaStream_t st)
         Epi ex = epi_none(m->Kp[l], m->err);
         ex.ldt = m->rows;
         ex.act = 2;
-        ex.z_in = m->z[l - 1];
+        ex.gp_in = m->gp[l - 1];
         ex.out_bf = m->g[l - 1];
         ex.out_bfT = m->gT[l - 1];
         ex.colsum = m->grads + m->b_off[l - 1];
@@ -821,13 +838,13 @@ extern "C" cuopo_status cuopo_mlp_create(cuopo_mlp **out, int n_in, int width, i
         if ((s = dalloc(m, &m->w_bf[l], (size_t)m->N[l] * m->Kp[l])) ||
             (s = dalloc(m, &m->wT_bf[l], (size_t)m->N[l] * m->Kp[l])))
             return fail(s);
-    m->z.resize(depth);
+    m->gp.resize(depth);
     m->h.resize(depth);
     m->hT.resize(depth);
     m->g.resize(depth);
     m->gT.resize(depth);
     for (int l = 0; l < depth; l++)
-        if ((s = dalloc(m, &m->z[l], R * width)) || (s = dalloc(m, &m->h[l], R * width)) ||
+        if ((s = dalloc(m, &m->gp[l], R * width)) || (s = dalloc(m, &m->h[l], R * width)) ||
             (s = dalloc(m, &m->hT[l], R * width)) || (s = dalloc(m, &m->g[l], R * width)) ||
             (s = dalloc(m, &m->gT[l], R * width)))
             return fail(s);
@@ -1176,4 +1193,98 @@ extern "C" cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, i
                                  (cudaStream_t)stream>>>((const float2 *)spec, n_t, n_modes,
                                                          (float)(1.0 / ((double)n_t * scale)), modes);
     return launch_check(cudaGetLastError(), "modes_from_spectrum");
+}
+
+/* ================================ warm-start fields from a band prediction */
+
+namespace {
+
+/* Layout of one prediction row (n_out = 512) of the band representation:
+ * [0, 128) magnitudes of the modes q0-64 .. q0+63, [128, 256) of the modes
+ * -q0-64 .. -q0+63, then 64 copies each of cos(Phi), sin(Phi), the band
+ * centre (q0 - n_t/4) / (n_t/4) and log10(P) (their means are used). */
+constexpr int BAND = 128;
+constexpr int BAND_ROW = 512;
+
+__global__ void fields_from_bands_kernel(const float *pred, int n_t, float scale, float2 *fields, int *centres)
+{
+    __shared__ float row[BAND_ROW];
+    __shared__ float2 coef[2 * BAND];
+    __shared__ float sc[2];
+    __shared__ int q0s;
+    const size_t inst = blockIdx.y;
+    const int t = threadIdx.x;   /* 256 threads */
+    for (int k = t; k < BAND_ROW; k += blockDim.x) row[k] = pred[inst * BAND_ROW + k];
+    __syncthreads();
+    if (t < 32) {
+        /* means of the four scalar groups, and the band power sum(max(a,0)^2) */
+        float m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int j = t; j < 64; j += 32)
+#pragma unroll
+            for (int g = 0; g < 4; g++) m[g] += row[2 * BAND + 64 * g + j];
+        for (int k = t; k < 2 * BAND; k += 32) {
+            const float a = fmaxf(row[k], 0.f);
+            m[4] += a * a;
+        }
+#pragma unroll
+        for (int g = 0; g < 5; g++)
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) m[g] += __shfl_xor_sync(0xffffffffu, m[g], d);
+        if (t == 0) {
+            const float quarter = (float)(n_t / 4);
+            int q0 = __float2int_rn(m[2] / 64.f * quarter + quarter);
+            q0 = max(BAND / 2, min(n_t / 2 - BAND / 2, q0));
+            q0s = q0;
+            const float phi = atan2f(m[1], m[0]);
+            const float p = exp10f(m[3] / 64.f);
+            const float amp = m[4] > 0.f ? sqrtf(p / m[4]) : 0.f;
+            sc[0] = amp * cosf(0.5f * phi);
+            sc[1] = amp * sinf(0.5f * phi);
+            if (centres) centres[inst] = q0;
+        }
+    }
+    __syncthreads();
+    for (int k = t; k < 2 * BAND; k += blockDim.x) {
+        const float a = fmaxf(row[k], 0.f);
+        coef[k] = make_float2(a * sc[0], a * sc[1]);   /* every pair c_q c_-q has phase Phi */
+    }
+    __syncthreads();
+    const int q0 = q0s;
+    const unsigned long long mask = (unsigned long long)n_t - 1;
+    const float inv = 2.0f / (float)n_t;
+    for (int n = blockIdx.x * blockDim.x + t; n < n_t; n += gridDim.x * blockDim.x) {
+        float sr, cr;
+        sincospif((float)((unsigned long long)n & mask) * inv, &sr, &cr);
+        float ar = 0.f, ai = 0.f;
+        for (int k0 = 0; k0 < 2 * BAND; k0 += 16) {
+            const long long q = (k0 < BAND) ? (long long)q0 - BAND / 2 + k0 : -(long long)q0 - BAND / 2 + (k0 - BAND);
+            const unsigned long long mm = ((unsigned long long)(q + 4LL * n_t) * (unsigned long long)n) & mask;
+            float s, c;
+            sincospif((float)mm * inv, &s, &c);
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const float2 v = coef[k0 + j];
+                ar += v.x * c - v.y * s;
+                ai += v.x * s + v.y * c;
+                const float c2 = c * cr - s * sr;
+                s = s * cr + c * sr;
+                c = c2;
+            }
+        }
+        fields[inst * n_t + n] = make_float2(scale * ar, scale * ai);
+    }
+}
+
+}  /* namespace */
+
+extern "C" cuopo_status cuopo_fields_from_bands(const float *pred, int count, int n_t, double scale, void *fields,
+                                                int *centres, void *stream)
+{
+    if (!pred || !fields || count < 1) return cuopo_fail(CUOPO_EINVAL, "fields_from_bands: bad argument");
+    if (n_t < 2 * BAND || (n_t & (n_t - 1)))
+        return cuopo_fail(CUOPO_EINVAL, "fields_from_bands: n_t must be a power of 2 >= 256");
+    dim3 grid((unsigned)((n_t + 255) / 256), (unsigned)count);
+    fields_from_bands_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(pred, n_t, (float)scale, (float2 *)fields,
+                                                                     centres);
+    return launch_check(cudaGetLastError(), "fields_from_bands");
 }

@@ -1,9 +1,20 @@
 """Learned warm start for CW sweeps.
 
 An MLP maps an instance's sweep parameters (pump ratio N, detuning delta,
-intracavity GDD, reflectivity R) to the 256 lowest Fourier modes of its
-steady-state signal; the batched solver then starts that instance from the
-predicted field instead of noise.  The network is the library's tensor-core
+intracavity GDD, reflectivity R) to a description of its steady-state
+signal; the batched solver then starts that instance from the predicted
+field instead of noise.  Two output representations (512 values each):
+
+* "low_modes": the 256 lowest Fourier modes (complex) of the steady state;
+* "band": the steady state of these detuned, dispersive cavities is a
+  signal/idler pair of bands around +-q0 (measured: >= 98 % of the power
+  within +-64 modes of the strongest pair for 90 % of the converged
+  instances, q0 up to ~3000 of 4096, reproducible between noise seeds to a
+  few modes), and the phase Phi of every pair product c_q c_-q is set by the
+  pump (coherent across the band to 0.998 and between seeds to 0.015 rad),
+  while the relative phases inside a band are not reproducible.  So the
+  network predicts the 2 x 128 band magnitudes, Phi, q0 and the power, and
+  the field is synthesised with every pair at phase Phi.  The network is the library's tensor-core
 MLP (cuopo_mlp_*, BF16 on tcgen05 with FP32 accumulation); the fields are
 made and read with the library's own FFT (cuopo_fft_c2c) and the
 spectrum/mode kernels.  A prediction is used only if it passes a one-round-
@@ -25,6 +36,8 @@ from ._lib import F32, check, load
 
 N_MODES = 256
 N_FEATURES = 4
+BAND = 128          # modes per band of the band representation
+MAG_SCALE = 8.0     # band magnitudes are stored with unit norm x MAG_SCALE
 WIDTH = 512
 DEPTH = 4
 # feature normalisation of the sweep's ranges to [-1, 1]
@@ -146,6 +159,41 @@ def fields_to_modes(fields, n_t: int, scale: float = 1.0, n_modes: int = N_MODES
     return modes
 
 
+def band_targets(fields, ps, n_t: int, stream=None):
+    """Training targets of the band representation from converged fields
+    (CUDA complex64 [count][n_t]) and their signal powers: the library's FFT
+    gives the modes c_q; the strongest signal/idler pair |c_q|^2 + |c_-q|^2
+    sets q0; rows as cuopo_fields_from_bands reads them."""
+    torch = _torch()
+    fields = fields.reshape(-1, n_t).contiguous()
+    count = fields.shape[0]
+    X = torch.empty_like(fields)
+    api.fft_c2c(fields, -1, out=X, stream=stream)
+    c = X / n_t
+    P = c.real ** 2 + c.imag ** 2
+    q = torch.arange(1, n_t // 2, device=fields.device)
+    pair = P[:, q] + P[:, (n_t - q) % n_t]
+    q0 = q[torch.argmax(pair, dim=1)].clamp(BAND // 2, n_t // 2 - BAND // 2)
+    k = torch.arange(BAND, device=fields.device)
+    ip = (q0[:, None] - BAND // 2 + k[None, :]) % n_t
+    im = (-q0[:, None] - BAND // 2 + k[None, :]) % n_t
+    cp = torch.gather(c, 1, ip)
+    cm = torch.gather(c, 1, im)
+    mags = torch.cat([cp.abs(), cm.abs()], dim=1)
+    mags = MAG_SCALE * mags / mags.norm(dim=1, keepdim=True).clamp_min(1e-30)
+    # pair k of the + band (q = q0-64+k) is mode 128-k of the - band
+    prod = (cp[:, 1:] * cm.flip(1)[:, :BAND - 1]).sum(dim=1)
+    phi = torch.angle(prod)
+    quarter = n_t / 4
+    y = torch.empty(count, 512, dtype=torch.float32, device=fields.device)
+    y[:, :2 * BAND] = mags
+    y[:, 256:320] = torch.cos(phi)[:, None]
+    y[:, 320:384] = torch.sin(phi)[:, None]
+    y[:, 384:448] = ((q0.float() - quarter) / quarter)[:, None]
+    y[:, 448:512] = torch.log10(torch.as_tensor(np.asarray(ps), dtype=torch.float32, device=fields.device))[:, None]
+    return y, q0
+
+
 def features(table, idx=None) -> np.ndarray:
     """Normalised network inputs [count][4] from a sweep table (n_thr, delta_rad, gdd_fs2, refl)."""
     raw = np.stack([np.asarray(table["n_thr"]), np.asarray(table["delta_rad"]), np.asarray(table["gdd_fs2"]),
@@ -174,6 +222,7 @@ class WarmStartModel:
         self.mlp = mlp
         self.amp_scale = float(amp_scale)
         self.meta = dict(meta or {})
+        self.kind = self.meta.get("kind", "low_modes")
 
     def save(self, path=MODEL_PATH) -> None:
         """Weights rounded to BF16 (the precision inference runs them at),
@@ -201,10 +250,24 @@ class WarmStartModel:
         return WarmStartModel(mlp, float(z["amp_scale"]), meta)
 
     def predict_modes(self, feats):
-        """Normalised features (numpy [count][4]) -> modes (CUDA float32, divided by amp_scale)."""
+        """Normalised features (numpy [count][4]) -> network outputs (CUDA float32 [count][512])."""
         torch = _torch()
         x = torch.from_numpy(np.ascontiguousarray(feats, np.float32)).cuda()
         return self.mlp.forward(x)
+
+    def fields(self, pred, n_t: int, stream=None):
+        """Network outputs -> initial signals (CUDA complex64 [count][n_t]) and the predicted powers."""
+        torch = _torch()
+        out = torch.empty(pred.shape[0], n_t, dtype=torch.complex64, device=pred.device)
+        if self.kind == "band":
+            check(load().cuopo_fields_from_bands(pred.contiguous().data_ptr(), pred.shape[0], n_t, 1.0,
+                                                 out.data_ptr(), None, _stream(stream)))
+            p0 = (10.0 ** pred[:, 448:512].double().mean(dim=1)).cpu().numpy()
+        else:
+            out = modes_to_fields(pred, n_t, self.amp_scale, stream=stream)
+            # predicted power: mean |A|^2 = sum |c_q|^2 (Parseval)
+            p0 = (self.amp_scale ** 2) * (pred.double() ** 2).sum(dim=1).cpu().numpy()
+        return out, p0
 
     def close(self):
         self.mlp.close()
@@ -213,10 +276,11 @@ class WarmStartModel:
 # ------------------------------------------------------------ data and training
 
 def generate_data(count: int, seed: int, n_t: int = 8192, n_z: int = 100, max_rt: int = 5000, tol: float = 1e-7,
-                  noise: float = 1e-15):
+                  noise: float = 1e-15, kind: str = "band"):
     """Solves a uniformly drawn CW sweep at one grid size from noise (the
     plain batched solver) and returns the converged instances' features and
-    steady-state modes (unscaled), with the run's bookkeeping."""
+    training targets (band rows, or unscaled low-order modes), with the
+    run's bookkeeping."""
     torch = _torch()
     from . import sweep
     base, insts, table = sweep.random_cw_sweep(count, seed, n_t_choices=(n_t,), n_z=n_z)
@@ -230,9 +294,13 @@ def generate_data(count: int, seed: int, n_t: int = 8192, n_z: int = 100, max_rt
     torch.cuda.synchronize()
     secs = time.perf_counter() - t0
     keep = np.flatnonzero((flags == 1) & (ps > 1e-20))
-    modes = fields_to_modes(sig.reshape(count, n_t)[torch.from_numpy(keep).cuda()], n_t)
-    return {"x": features(table, keep), "y": modes.cpu().numpy(), "ps": ps[keep], "rts": rts, "flags": flags,
-            "seconds": secs, "count": count, "seed": seed, "n_t": n_t}
+    conv = sig.reshape(count, n_t)[torch.from_numpy(keep).cuda()]
+    if kind == "band":
+        y, _ = band_targets(conv, ps[keep], n_t)
+    else:
+        y = fields_to_modes(conv, n_t)
+    return {"x": features(table, keep), "y": y.cpu().numpy(), "ps": ps[keep], "rts": rts, "flags": flags,
+            "seconds": secs, "count": count, "seed": seed, "n_t": n_t, "kind": kind}
 
 
 def train(mlp: MLP, x: np.ndarray, y: np.ndarray, steps: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
@@ -276,13 +344,16 @@ def warm_start(model: WarmStartModel, batch: "api.Batch", insts, table, noise: f
     batch.seed_noise(noise, stream=stream)
     batch.get_signal(sig_noise, stream=stream)
     trial = torch.empty_like(sig_noise)
+    p0 = np.zeros(len(insts))
     for n in sorted(set(n_ts.tolist())):
         sel = np.flatnonzero(n_ts == n)
-        f = modes_to_fields(pred[torch.from_numpy(sel).cuda()], int(n), model.amp_scale, stream=stream)
-        for j, k in enumerate(sel):
-            trial[offs[k]:offs[k + 1]] = f[j]
-    # predicted power: mean |A|^2 = sum |c_q|^2 (Parseval)
-    p0 = (model.amp_scale ** 2) * (pred.double() ** 2).sum(dim=1).cpu().numpy()
+        f, p = model.fields(pred[torch.from_numpy(sel).cuda()], int(n), stream=stream)
+        p0[sel] = p
+        if np.all(np.diff(offs[sel]) == n) and len(sel) > 0:
+            trial[offs[sel[0]]:offs[sel[-1] + 1]] = f.reshape(-1)
+        else:
+            for j, k in enumerate(sel):
+                trial[offs[k]:offs[k + 1]] = f[j]
     batch.set_signal(trial, stream=stream)
     batch.reset(stream=stream)
     batch.step(1, 1, 0.0, 1, stream=stream)
@@ -376,21 +447,27 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-count", type=int, default=512)
     ap.add_argument("--eval-seed", type=int, default=7)
+    ap.add_argument("--kind", choices=["band", "low_modes"], default="band")
+    ap.add_argument("--check-tol", type=float, default=0.1)
     ap.add_argument("--out", type=str, default=str(MODEL_PATH))
     ap.add_argument("--summary", type=str, default="")
     a = ap.parse_args()
     summary = {}
     if a.cmd == "train":
-        d = generate_data(a.count, a.seed, n_t=a.n_t)
+        d = generate_data(a.count, a.seed, n_t=a.n_t, kind=a.kind)
         y = d["y"]
-        # outputs scaled so that a typical steady state has unit norm over its modes
-        amp = float(np.sqrt(np.mean(np.sum(y.astype(np.float64) ** 2, axis=1)))) if y.size else 1.0
+        if a.kind == "band":
+            amp = 1.0
+        else:
+            # outputs scaled so that a typical steady state has unit norm over its modes
+            amp = float(np.sqrt(np.mean(np.sum(y.astype(np.float64) ** 2, axis=1)))) if y.size else 1.0
         mlp = MLP(max_batch=a.batch, seed=a.seed)
         t0 = time.perf_counter()
         losses = train(mlp, d["x"], y / amp, a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
         train_s = time.perf_counter() - t0
-        model = WarmStartModel(mlp, amp, {"count": a.count, "converged": int(len(y)), "seed": a.seed,
-                                          "n_t": a.n_t, "steps": a.steps, "batch": a.batch, "lr": a.lr})
+        model = WarmStartModel(mlp, amp, {"kind": a.kind, "count": a.count, "converged": int(len(y)),
+                                          "seed": a.seed, "n_t": a.n_t, "steps": a.steps, "batch": a.batch,
+                                          "lr": a.lr, "data_gpu_seconds": round(d["seconds"], 1)})
         model.save(a.out)
         summary.update(data={"instances": a.count, "converged_states": int(len(y)), "seconds": d["seconds"],
                              "n_t": a.n_t},
@@ -398,7 +475,7 @@ def main():
                               "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:]))},
                        amp_scale=amp)
     model = WarmStartModel.load(a.out)
-    summary["eval"] = evaluate(model, a.eval_count, a.eval_seed, n_t=a.n_t)
+    summary["eval"] = evaluate(model, a.eval_count, a.eval_seed, n_t=a.n_t, check_tol=a.check_tol)
     txt = json.dumps(summary, indent=1)
     print(txt)
     if a.summary:

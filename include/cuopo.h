@@ -424,6 +424,17 @@ cuopo_status cuopo_fields_from_modes(const float *modes, int count, int n_modes,
                                      void *stream);
 cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, int n_t, int n_modes, double scale, float *modes,
                                        void *stream);
+/* Warm-start fields from the band representation: each row of `pred` (512
+ * floats, an MLP output) holds the magnitudes of the 128 modes around +q0
+ * ([0,128): q0-64 .. q0+63) and around -q0 ([128,256): -q0-64 .. -q0+63),
+ * then 64 copies each of cos(Phi), sin(Phi), (q0 - n_t/4)/(n_t/4) and
+ * log10(P).  The field is scale * sum_q c_q exp(+2 pi i q n / n_t) with
+ * |c_q| proportional to max(magnitude, 0), total power P (the means of the
+ * copies; q0 rounded and clamped to [64, n_t/2 - 64]) and every mode of
+ * phase Phi/2, so that each signal-idler pair c_q c_-q has the phase Phi.
+ * centres (device, may be NULL) gets each instance's q0. */
+cuopo_status cuopo_fields_from_bands(const float *pred, int count, int n_t, double scale, void *fields, int *centres,
+                                     void *stream);
 
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (best of 3
  * launches each of a scalar and a packed FP32x2 FMA-chain kernel over every

@@ -9,8 +9,9 @@ difference check of its own gradients (tests/test_mlp_oracle.py), not by
 reference vectors.
 
 With emulate_bf16=True the values that the GPU stores in BF16 are rounded
-to BF16 at the same points: the input, the weights, the pre-activations z
-(read back for GELU'), the activations h, the output gradient and every
+to BF16 at the same points: the input, the weights, the derivative
+GELU'(z) of every hidden pre-activation (stored by the forward pass for the
+backward one), the activations h, the output gradient and every
 back-propagated gradient (the bias gradients sum the rounded values).  Sums
 are exact (float64) either way, so the remaining difference from the GPU is
 its FP32 accumulation order and FP32 GELU.
@@ -72,12 +73,12 @@ def forward(params, x, dims, emulate_bf16: bool = True):
     r = bf16 if emulate_bf16 else (lambda a: np.asarray(a, np.float64))
     layers = unpack(np.asarray(params, np.float64), dims)
     a = r(x)
-    cache = {"a": [a], "z": []}
+    cache = {"a": [a], "gp": []}
     for l, (W, b) in enumerate(layers):
         z = a @ r(W).T + b
         if l == len(layers) - 1:
             return z, cache
-        cache["z"].append(r(z))
+        cache["gp"].append(r(gelu_grad(z)))
         a = r(gelu(z))
         cache["a"].append(a)
     raise AssertionError("unreachable")
@@ -102,7 +103,7 @@ def loss_and_grads(params, x, t, dims, emulate_bf16: bool = True):
         grads[l] = (gW, gb)
         if l == 0:
             break
-        g = r((g @ r(W)) * gelu_grad(cache["z"][l - 1]))
+        g = r((g @ r(W)) * cache["gp"][l - 1])
     return loss, pack(grads)
 
 

@@ -172,3 +172,39 @@ def test_modes_fields_round_trip(n_t):
     assert _rel(back_neg.cpu().numpy(), m) < 1e-5
     # the field itself: its mean is mode 0 times the scale
     assert abs(f.mean(dim=1)[0].item() - 2.0 * complex(m[0, 256], m[0, 257])) < 1e-4
+
+
+def test_band_targets_and_synthesis_round_trip():
+    """A field made of two bands around +-q0 whose pairs c_q c_-q share the
+    phase Phi: band_targets recovers q0, Phi and the power, and
+    cuopo_fields_from_bands rebuilds a field with the same band power
+    spectrum, power and pair phase (FFT of the library)."""
+    from cuopo_b200 import api
+    from cuopo_b200 import warmstart as ws
+    n_t, q0, phi, P = 8192, 2500, 0.9, 0.6
+    rng = np.random.default_rng(4)
+    k = np.arange(ws.BAND) - ws.BAND // 2
+    mag = np.exp(-(k / 20.0) ** 2)
+    spec = np.zeros(n_t, np.complex128)
+    psi = rng.uniform(-np.pi, np.pi, ws.BAND)          # in-band relative phases (not predicted)
+    spec[(q0 + k) % n_t] = mag * np.exp(1j * (phi / 2 + psi))
+    spec[(-q0 - k) % n_t] = mag * np.exp(1j * (phi / 2 - psi))
+    spec *= np.sqrt(P / np.sum(np.abs(spec) ** 2))
+    field = np.fft.ifft(spec) * n_t                    # A[n] = sum_q c_q e^{+2 pi i q n / N}
+    F = torch.from_numpy(field.astype(np.complex64)).cuda()[None, :]
+    y, q_found = ws.band_targets(F, np.array([P]), n_t)
+    assert int(q_found[0]) == q0
+    yy = y.cpu().numpy()[0]
+    assert abs(np.arctan2(yy[320:384].mean(), yy[256:320].mean()) - phi) < 1e-4
+    assert abs(10 ** yy[448:512].mean() - P) < 1e-5 * P
+    out = torch.empty(1, n_t, dtype=torch.complex64, device="cuda")
+    from cuopo_b200._lib import check, load
+    check(load().cuopo_fields_from_bands(y.data_ptr(), 1, n_t, 1.0, out.data_ptr(), None,
+                                         torch.cuda.current_stream().cuda_stream))
+    c = api.fft_c2c(out.contiguous(), -1).cpu().numpy()[0] / n_t
+    assert abs(np.sum(np.abs(c) ** 2) - P) < 1e-4 * P
+    got = np.abs(c[(q0 + k) % n_t])
+    want = np.abs(spec[(q0 + k) % n_t])
+    assert _rel(got, want) < 1e-4
+    pairs = c[(q0 + k) % n_t] * c[(-q0 - k) % n_t]
+    assert abs(np.angle(pairs.sum()) - phi) < 1e-4
