@@ -182,7 +182,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 
 /* -------------------------------------------------------- GELU (erf form) */
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+/* GELU(z) = z Phi(z) and GELU'(z) = Phi(z) + z phi(z), with
+ * Phi(z) = (1 + erf(z / sqrt 2)) / 2 and phi(z) = exp(-z^2 / 2) / sqrt(2 pi).
+ * erf(x), x >= 0, by Abramowitz & Stegun 7.1.26 (Handbook of Mathematical
+ * Functions, 1964): 1 - (a1 t + ... + a5 t^5) exp(-x^2), t = 1 / (1 + p x),
+ * absolute error <= 1.5e-7 -- far below the BF16 rounding of the stored
+ * values -- and its exp(-x^2) = exp(-z^2/2) is also phi's. */
+__device__ __forceinline__ void gelu_and_grad(float z, float &h, float &gp)
+{
+    const float x = fabsf(z) * 0.70710678118654752f;
+    const float e = __expf(-0.5f * z * z);
+    const float t = __fdividef(1.0f, 1.0f + 0.3275911f * x);
+    const float poly =
+        t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f))));
+    const float erf_abs = 1.0f - poly * e;
+    const float phi_cdf = 0.5f + 0.5f * copysignf(erf_abs, z);
+    h = z * phi_cdf;
+    gp = phi_cdf + z * 0.39894228040143268f * e;
+}
 
 
 /* ------------------------------------------------------------ epilogue */
@@ -245,21 +262,10 @@ __device__ __forceinline__ void epilogue32(const Epi &ep, int row, int col, floa
     }
     const size_t o = (size_t)row * ep.ldo + col;
     if (ep.act == 1) {
-        if (ep.gp_out) {
-            /* GELU and its derivative from one erf: h = z Phi(z), h' = Phi(z) + z phi(z) */
-            float gp[32];
+        float gp[32];
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-                const float z = v[j];
-                const float ph = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-                gp[j] = ph + z * 0.39894228040143268f * expf(-0.5f * z * z);
-                v[j] = z * ph;
-            }
-            if (store) store_bf16x32(ep.gp_out + o, gp);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 32; j++) v[j] = gelu(v[j]);
-        }
+        for (int j = 0; j < 32; j++) gelu_and_grad(v[j], v[j], gp[j]);
+        if (ep.gp_out && store) store_bf16x32(ep.gp_out + o, gp);
     } else if (ep.act == 2) {
         float gp[32];
         load_bf16x32(ep.gp_in + o, gp);
@@ -541,16 +547,18 @@ __global__ void pack_kernel(const PackArgs a)
 /* Mean squared error over batch x n_out and its gradient 2 (y - t) / (batch
  * n_out) (zero on rows >= batch), stored as g [rows][n_out] and g^T
  * [n_out][ldt] (BF16); bias gradient += column sums of the BF16 g; loss +=
- * the batch's mean.  Block: n_out threads x 32 rows. */
+ * the batch's mean.  Block: n_out threads x MSE_ROWS rows (each thread
+ * writes its column's MSE_ROWS values of g^T as 16-byte stores). */
+constexpr int MSE_ROWS = 16;
 __global__ void mse_kernel(const float *y, const float *tgt, bf16 *g, bf16 *gT, float *db, float *loss, int batch,
                            int n_out, int ldt)
 {
-    const int j = threadIdx.x, r0 = blockIdx.x * 32;
+    const int j = threadIdx.x, r0 = blockIdx.x * MSE_ROWS;
     const float scale = 2.0f / ((float)batch * (float)n_out);
     float csum = 0.f, lsum = 0.f;
-    uint32_t packed[16];
+    uint32_t packed[MSE_ROWS / 2];
 #pragma unroll
-    for (int q = 0; q < 32; q += 2) {
+    for (int q = 0; q < MSE_ROWS; q += 2) {
         float gv[2];
 #pragma unroll
         for (int u = 0; u < 2; u++) {
@@ -569,7 +577,8 @@ __global__ void mse_kernel(const float *y, const float *tgt, bf16 *g, bf16 *gT, 
     }
     uint4 *dst = reinterpret_cast<uint4 *>(gT + (size_t)j * ldt + r0);
 #pragma unroll
-    for (int q = 0; q < 4; q++) dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
+    for (int q = 0; q < MSE_ROWS / 8; q++)
+        dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
     atomicAdd(db + j, csum);
     __shared__ float part[32];
 #pragma unroll
@@ -618,13 +627,22 @@ __global__ void adam_kernel(const AdamArgs a, long total)
     int s = 0;
     while (s + 1 < a.nseg && i >= a.seg[s + 1].off) s++;
     const Seg &sg = a.seg[s];
-    if (sg.Kp > 0) {
-        const long li = i - sg.off;
-        const int n = (int)(li / sg.Kp), k = (int)(li % sg.Kp);
-        const bf16 b = __float2bfloat16_rn(p);
-        sg.w[li] = b;
-        sg.wT[(size_t)k * sg.N + n] = b;
-    }
+    if (sg.Kp > 0) sg.w[i - sg.off] = __float2bfloat16_rn(p);
+}
+
+/* W^T [Kp][N] from W [N][Kp] (BF16) through 32 x 32 shared-memory tiles, so
+ * that both the reads and the writes are coalesced; blockIdx.z = weight
+ * segment (a.seg[2 l]). */
+__global__ void transpose_weights_kernel(const AdamArgs a)
+{
+    __shared__ bf16 tile[32][33];
+    const Seg &sg = a.seg[2 * blockIdx.z];
+    const int n0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    if (n0 >= sg.N || k0 >= sg.Kp) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;   /* 32 x 8 */
+    for (int r = ty; r < 32; r += 8) tile[r][tx] = sg.w[(size_t)(n0 + r) * sg.Kp + k0 + tx];
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) sg.wT[(size_t)(k0 + r) * sg.N + n0 + tx] = tile[tx][r];
 }
 
 }  /* namespace */
@@ -706,7 +724,7 @@ cuopo_status backward(cuopo_mlp *m, int batch, int rows_used, cudaStream_t st)
     if (e == cudaSuccess) e = cudaMemsetAsync(m->loss, 0, sizeof(float), st);
     if (e != cudaSuccess) return cuda_err(e, "mlp: memset");
     const int Lo = m->L - 1;
-    mse_kernel<<<rows_used / 32, m->n_out, 0, st>>>(m->y, m->tgt, m->g_out, m->g_outT, m->grads + m->b_off[Lo],
+    mse_kernel<<<rows_used / MSE_ROWS, m->n_out, 0, st>>>(m->y, m->tgt, m->g_out, m->g_outT, m->grads + m->b_off[Lo],
                                                    m->loss, batch, m->n_out, m->rows);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "mlp: loss kernel");
     for (int l = Lo; l >= 0; l--) {
@@ -743,7 +761,16 @@ cuopo_status run_adam(cuopo_mlp *m, int update, cudaStream_t st)
     a.update = update;
     const int tpb = 256;
     adam_kernel<<<(unsigned)((m->P + tpb - 1) / tpb), tpb, 0, st>>>(a, m->P);
-    return launch_check(cudaGetLastError(), "mlp: adam kernel");
+    cuopo_status s = launch_check(cudaGetLastError(), "mlp: adam kernel");
+    if (s != CUOPO_OK) return s;
+    int maxN = 0, maxK = 0;
+    for (int l = 0; l < m->L; l++) {
+        maxN = m->N[l] > maxN ? m->N[l] : maxN;
+        maxK = m->Kp[l] > maxK ? m->Kp[l] : maxK;
+    }
+    transpose_weights_kernel<<<dim3((unsigned)(maxK / 32), (unsigned)(maxN / 32), (unsigned)m->L), dim3(32, 8), 0,
+                               st>>>(a);
+    return launch_check(cudaGetLastError(), "mlp: weight transpose kernel");
 }
 
 cuopo_status pack(cuopo_mlp *m, const float *x, const float *t, int batch, int rows_used, bool train, float lr,
@@ -1202,7 +1229,8 @@ namespace {
 /* Layout of one prediction row (n_out = 512) of the band representation:
  * [0, 128) magnitudes of the modes q0-64 .. q0+63, [128, 256) of the modes
  * -q0-64 .. -q0+63, then 64 copies each of cos(Phi), sin(Phi), the band
- * centre (q0 - n_t/4) / (n_t/4) and log10(P) (their means are used). */
+ * centre as 2 (q0 / (n_t/2))^2 - 1 (q0^2 is close to linear in the cavity
+ * detuning) and log10(P) (their means are used). */
 constexpr int BAND = 128;
 constexpr int BAND_ROW = 512;
 
@@ -1231,8 +1259,8 @@ __global__ void fields_from_bands_kernel(const float *pred, int n_t, float scale
 #pragma unroll
             for (int d = 16; d > 0; d >>= 1) m[g] += __shfl_xor_sync(0xffffffffu, m[g], d);
         if (t == 0) {
-            const float quarter = (float)(n_t / 4);
-            int q0 = __float2int_rn(m[2] / 64.f * quarter + quarter);
+            const float u = fmaxf(0.5f * (m[2] / 64.f + 1.0f), 0.f);
+            int q0 = __float2int_rn(sqrtf(u) * (float)(n_t / 2));
             q0 = max(BAND / 2, min(n_t / 2 - BAND / 2, q0));
             q0s = q0;
             const float phi = atan2f(m[1], m[0]);

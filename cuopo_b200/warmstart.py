@@ -159,6 +159,18 @@ def fields_to_modes(fields, n_t: int, scale: float = 1.0, n_modes: int = N_MODES
     return modes
 
 
+def centre_code(q0, n_t: int):
+    """The band centre as the network predicts it: 2 (q0 / (n_t/2))^2 - 1
+    (q0^2 is close to linear in the cavity detuning; the synthesis kernel
+    inverts it)."""
+    return 2.0 * (q0 / (n_t / 2)) ** 2 - 1.0
+
+
+def centre_decode(code, n_t: int):
+    return np.clip(np.rint(np.sqrt(np.maximum(0.5 * (np.asarray(code) + 1.0), 0.0)) * (n_t / 2)),
+                   BAND // 2, n_t // 2 - BAND // 2)
+
+
 def band_targets(fields, ps, n_t: int, stream=None):
     """Training targets of the band representation from converged fields
     (CUDA complex64 [count][n_t]) and their signal powers: the library's FFT
@@ -184,12 +196,11 @@ def band_targets(fields, ps, n_t: int, stream=None):
     # pair k of the + band (q = q0-64+k) is mode 128-k of the - band
     prod = (cp[:, 1:] * cm.flip(1)[:, :BAND - 1]).sum(dim=1)
     phi = torch.angle(prod)
-    quarter = n_t / 4
     y = torch.empty(count, 512, dtype=torch.float32, device=fields.device)
     y[:, :2 * BAND] = mags
     y[:, 256:320] = torch.cos(phi)[:, None]
     y[:, 320:384] = torch.sin(phi)[:, None]
-    y[:, 384:448] = ((q0.float() - quarter) / quarter)[:, None]
+    y[:, 384:448] = centre_code(q0.float(), n_t)[:, None]
     y[:, 448:512] = torch.log10(torch.as_tensor(np.asarray(ps), dtype=torch.float32, device=fields.device))[:, None]
     return y, q0
 
@@ -322,7 +333,8 @@ def train(mlp: MLP, x: np.ndarray, y: np.ndarray, steps: int, batch: int = 4096,
         idx = torch.randint(0, n, (b,), generator=g, device="cuda")
         torch.index_select(X, 0, idx, out=xb)
         torch.index_select(Y, 0, idx, out=yb)
-        mlp.train_step(xb, yb, lr, loss=losses[s])
+        # the learning rate drops 10x for the last 30 % of the steps
+        mlp.train_step(xb, yb, lr if s < 0.7 * steps else 0.1 * lr, loss=losses[s])
     mlp.status()
     out = losses.cpu().numpy()
     return out if not log_every else out[::log_every]
@@ -331,7 +343,7 @@ def train(mlp: MLP, x: np.ndarray, y: np.ndarray, steps: int, batch: int = 4096,
 # ------------------------------------------------------------ warm-started solve
 
 def warm_start(model: WarmStartModel, batch: "api.Batch", insts, table, noise: float = 1e-15,
-               check_tol: float = 0.1, p_min: float = 1e-12, stream=None) -> dict:
+               check_tol: float = 0.5, p_min: float = 1e-12, stream=None) -> dict:
     """Sets every instance's initial signal: the network's predicted steady
     state where it passes the first-round-trip check, else the instance's
     seeded noise (as a plain solve).  Leaves the batch reset at round trip 0.
@@ -369,7 +381,7 @@ def warm_start(model: WarmStartModel, batch: "api.Batch", insts, table, noise: f
 
 
 def solve_sweep(base, insts, table, model: WarmStartModel | None, max_rt: int = 5000, tol: float = 1e-7,
-                noise: float = 1e-15, check_tol: float = 0.1) -> dict:
+                noise: float = 1e-15, check_tol: float = 0.5, return_fields: bool = False) -> dict:
     """One sweep solved to the convergence rule, from noise (model None) or
     warm-started; CUDA-event time of everything after batch creation
     (prediction, field synthesis, the check round trip, the solve)."""
@@ -391,44 +403,64 @@ def solve_sweep(base, insts, table, model: WarmStartModel | None, max_rt: int = 
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         ps, rts, flags = b.results()
-    out = {"ms": ms, "ps": ps, "rts": rts, "flags": flags}
+        fields = None
+        if return_fields:
+            fields = torch.empty(b.total, dtype=torch.complex64, device="cuda")
+            b.get_signal(fields)
+    out = {"ms": ms, "ps": ps, "rts": rts, "flags": flags, "fields": fields}
     if ws is not None:
         out.update(accept=ws["accept"], resid=ws["resid"])
     return out
 
 
+def _arm(r, count):
+    conv = r["flags"] == 1
+    n = int(np.sum(conv))
+    out = {"seconds": r["ms"] * 1e-3, "converged": n, "round_trips": int(np.sum(r["rts"])),
+           "solves_per_s": count / (r["ms"] * 1e-3), "converged_solves_per_s": n / (r["ms"] * 1e-3),
+           "median_rts_converged": float(np.median(r["rts"][conv])) if n else None}
+    if "accept" in r:
+        acc = r["accept"]
+        out.update(accepted=int(np.sum(acc)), accepted_converged=int(np.sum(acc & conv)),
+                   median_rts_accepted_converged=float(np.median(r["rts"][acc & conv])) if np.any(acc & conv)
+                   else None)
+    return out
+
+
+def _judge(r, ref):
+    both = (ref["flags"] == 1) & (r["flags"] == 1) & (ref["ps"] > 1e-20)
+    err = np.abs(r["ps"][both] - ref["ps"][both]) / ref["ps"][both]
+    return {"instances": int(np.sum(both)), "max_rel_err_ps": float(np.max(err)) if err.size else None,
+            "median_rel_err_ps": float(np.median(err)) if err.size else None,
+            "frac_within_1e-5": float(np.mean(err <= 1e-5)) if err.size else None}
+
+
 def evaluate(model: WarmStartModel, count: int, seed: int, n_t: int = 8192, n_z: int = 100, max_rt: int = 5000,
-             tol: float = 1e-7, check_tol: float = 0.1) -> dict:
-    """Held-out comparison on a freshly drawn sweep: plain (noise-seeded)
-    against warm-started solves of the same instances with the same solver
-    and rule.  The warm-started final signal power of every instance that
-    converged in both is judged against the plain solve's."""
+             tol: float = 1e-7, check_tol: float = 0.5, control_noise: float = 1e-10) -> dict:
+    """Held-out comparison on a freshly drawn sweep, the same instances,
+    solver and rule in three arms: plain (noise-seeded, sigma 1e-15), warm
+    (the network's prediction where it passes the first-round-trip check,
+    else the same noise) and a control without the network (noise seeded
+    with sigma `control_noise`, which also skips part of the build-up).  The
+    final signal power of every instance that converged in an arm and in the
+    plain solve is judged against the plain solve's."""
     from . import sweep
     base, insts, table = sweep.random_cw_sweep(count, seed, n_t_choices=(n_t,), n_z=n_z)
     plain = solve_sweep(base, insts, table, None, max_rt, tol)
     warm = solve_sweep(base, insts, table, model, max_rt, tol, check_tol=check_tol)
-    both = (plain["flags"] == 1) & (warm["flags"] == 1) & (plain["ps"] > 1e-20)
-    err = np.abs(warm["ps"][both] - plain["ps"][both]) / plain["ps"][both]
-    conv_p, conv_w = int(np.sum(plain["flags"] == 1)), int(np.sum(warm["flags"] == 1))
-    acc = warm["accept"]
-    return {
-        "count": count, "seed": seed, "n_t": n_t, "max_rt": max_rt, "tol": tol,
-        "plain": {"seconds": plain["ms"] * 1e-3, "converged": conv_p, "round_trips": int(np.sum(plain["rts"])),
-                  "solves_per_s": count / (plain["ms"] * 1e-3), "converged_solves_per_s": conv_p / (plain["ms"] * 1e-3),
-                  "median_rts_converged": float(np.median(plain["rts"][plain["flags"] == 1])) if conv_p else None},
-        "warm": {"seconds": warm["ms"] * 1e-3, "converged": conv_w, "round_trips": int(np.sum(warm["rts"])),
-                 "solves_per_s": count / (warm["ms"] * 1e-3), "converged_solves_per_s": conv_w / (warm["ms"] * 1e-3),
-                 "median_rts_converged": float(np.median(warm["rts"][warm["flags"] == 1])) if conv_w else None,
-                 "accepted": int(np.sum(acc)),
-                 "accepted_converged": int(np.sum(acc & (warm["flags"] == 1))),
-                 "median_rts_accepted_converged": float(np.median(warm["rts"][acc & (warm["flags"] == 1)]))
-                 if np.any(acc & (warm["flags"] == 1)) else None},
-        "gain_converged_solves_per_s": (conv_w / warm["ms"]) / (conv_p / plain["ms"]) if conv_p else None,
-        "judged_by_plain": {"instances": int(np.sum(both)),
-                            "max_rel_err_ps": float(np.max(err)) if err.size else None,
-                            "median_rel_err_ps": float(np.median(err)) if err.size else None,
-                            "frac_within_1e-5": float(np.mean(err <= 1e-5)) if err.size else None},
-    }
+    ctrl = solve_sweep(base, insts, table, None, max_rt, tol, noise=control_noise) if control_noise else None
+    conv_p = int(np.sum(plain["flags"] == 1))
+    rate = lambda r: int(np.sum(r["flags"] == 1)) / r["ms"]
+    out = {"count": count, "seed": seed, "n_t": n_t, "max_rt": max_rt, "tol": tol, "check_tol": check_tol,
+           "model": model.kind, "plain": _arm(plain, count), "warm": _arm(warm, count),
+           "gain_converged_solves_per_s": rate(warm) / rate(plain) if conv_p else None,
+           "warm_judged_by_plain": _judge(warm, plain)}
+    if ctrl is not None:
+        out["control_noise"] = control_noise
+        out["control"] = _arm(ctrl, count)
+        out["control_gain_converged_solves_per_s"] = rate(ctrl) / rate(plain) if conv_p else None
+        out["control_judged_by_plain"] = _judge(ctrl, plain)
+    return out
 
 
 def main():
@@ -438,7 +470,10 @@ def main():
     import argparse
     import json
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "eval", "steps"],
+                    help="train: data + training + held-out comparison; eval: comparison with the saved model; "
+                         "steps: --steps training steps of a fresh network on random data (kernel timing and "
+                         "profiling)")
     ap.add_argument("--count", type=int, default=4096, help="sweep instances solved for training data")
     ap.add_argument("--seed", type=int, default=100)
     ap.add_argument("--n-t", type=int, default=8192)
@@ -448,13 +483,36 @@ def main():
     ap.add_argument("--eval-count", type=int, default=512)
     ap.add_argument("--eval-seed", type=int, default=7)
     ap.add_argument("--kind", choices=["band", "low_modes"], default="band")
-    ap.add_argument("--check-tol", type=float, default=0.1)
+    ap.add_argument("--save-data", type=str, default="", help="write the generated training set (npz)")
+    ap.add_argument("--data", type=str, default="", help="train on a saved training set instead of solving")
+    ap.add_argument("--check-tol", type=float, default=0.5)
     ap.add_argument("--out", type=str, default=str(MODEL_PATH))
     ap.add_argument("--summary", type=str, default="")
     a = ap.parse_args()
     summary = {}
+    if a.cmd == "steps":
+        torch = _torch()
+        mlp = MLP(max_batch=a.batch, seed=a.seed)
+        x = torch.rand(a.batch, N_FEATURES, device="cuda") * 2 - 1
+        t = torch.randn(a.batch, 2 * N_MODES, device="cuda")
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(a.steps):
+            mlp.train_step(x, t, a.lr)
+        ev[1].record()
+        torch.cuda.synchronize()
+        mlp.status()
+        print(json.dumps({"steps": a.steps, "batch": a.batch, "ms_per_step": ev[0].elapsed_time(ev[1]) / a.steps}))
+        return
     if a.cmd == "train":
-        d = generate_data(a.count, a.seed, n_t=a.n_t, kind=a.kind)
+        if a.data:
+            z = np.load(a.data)
+            d = {k: z[k] for k in z.files}
+            d["seconds"] = float(d["seconds"])
+        else:
+            d = generate_data(a.count, a.seed, n_t=a.n_t, kind=a.kind)
+            if a.save_data:
+                np.savez_compressed(a.save_data, x=d["x"], y=d["y"], ps=d["ps"], seconds=d["seconds"])
         y = d["y"]
         if a.kind == "band":
             amp = 1.0

@@ -427,7 +427,7 @@ cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, int n_t, int
 /* Warm-start fields from the band representation: each row of `pred` (512
  * floats, an MLP output) holds the magnitudes of the 128 modes around +q0
  * ([0,128): q0-64 .. q0+63) and around -q0 ([128,256): -q0-64 .. -q0+63),
- * then 64 copies each of cos(Phi), sin(Phi), (q0 - n_t/4)/(n_t/4) and
+ * then 64 copies each of cos(Phi), sin(Phi), 2 (q0 / (n_t/2))^2 - 1 and
  * log10(P).  The field is scale * sum_q c_q exp(+2 pi i q n / n_t) with
  * |c_q| proportional to max(magnitude, 0), total power P (the means of the
  * copies; q0 rounded and clamped to [64, n_t/2 - 64]) and every mode of
