@@ -83,6 +83,7 @@ _d = C.c_double
 SIGNATURES = {
     "cuopo_inputs_default": (None, [C.POINTER(Inputs)]),
     "cuopo_derive_params": (_i, [C.POINTER(Inputs), C.POINTER(Params), C.POINTER(Info)]),
+    "cuopo_derive_params_device": (_i, [_vp, _i, _vp, _vp, _vp]),
     "cuopo_sellmeier": (C.c_float, [_i, _i, C.c_float, C.c_float]),
     "cuopo_phase_matching_temp": (C.c_float, [_i, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
     "cuopo_make_grids": (_i, [_i, _d, _vp, _vp]),

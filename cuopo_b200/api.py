@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import CW, F32, F64, NS, PPLN, SPPLT, Info, Inputs, Params, check, load
+from ._lib import CW, F32, F64, NS, OK, PPLN, SPPLT, CuopoError, Info, Inputs, Params, check, load
 
 
 def default_inputs(**kw) -> Inputs:
@@ -35,6 +35,23 @@ def derive_params(inputs: Inputs) -> tuple[Params, Info]:
     p, info = Params(), Info()
     check(load().cuopo_derive_params(C.byref(inputs), C.byref(p), C.byref(info)))
     return p, info
+
+
+def derive_params_device(inputs, stream=None) -> list[Params]:
+    """cuopo_derive_params_device: a list of Inputs derived on the GPU in one
+    launch (one warp per instance).  Raises if any instance is invalid."""
+    import torch
+    n = len(inputs)
+    arr = (Inputs * n)(*inputs)
+    d_in = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).cuda()
+    d_out = torch.zeros(n * C.sizeof(Params), dtype=torch.uint8, device="cuda")
+    d_st = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    check(load().cuopo_derive_params_device(d_in.data_ptr(), n, d_out.data_ptr(), d_st.data_ptr(), _stream(stream)))
+    st = d_st.cpu().numpy()
+    if np.any(st != OK):
+        raise CuopoError(int(st[st != OK][0]), f"derive_params_device: instance {int(np.flatnonzero(st != OK)[0])} invalid")
+    raw = d_out.cpu().numpy().tobytes()
+    return list((Params * n).from_buffer_copy(raw))
 
 
 def make_grids(n_t: int, t_rt: float) -> tuple[np.ndarray, np.ndarray]:

@@ -25,7 +25,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CC_FLAGS = ["-O2", "-fPIC", "-std=c11", "-Wall", "-Wextra", "-fvisibility=hidden", "-I" + str(INCLUDE),
             "-I" + str(CSRC)]
 
-CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu", "probe.cu", "mlp.cu"]
+CU_SOURCES = ["solver.cu", "noise.cu", "fft_api.cu", "probe.cu", "mlp.cu", "params_dev.cu"]
+# per-file nvcc flags: the device set-up keeps the host's float rounding (no FMA contraction)
+CU_EXTRA = {"params_dev.cu": ["-fmad=false"]}
 C_SOURCES = ["params.c", "dat_io.c"]
 BIN = HERE / "bin"
 CLI = BIN / "cuopo"
@@ -72,7 +74,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         obj = OBJ / (s + ".o")
         objs.append(obj)
         if force or _stale(obj, _deps(src)):
-            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+            cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, *CU_EXTRA.get(s, []), "-c", str(src), "-o", str(obj)]
             if ptxas_verbose:
                 cmd.insert(1, "-Xptxas=-v")
             jobs.append(cmd)

@@ -128,6 +128,17 @@ void cuopo_inputs_default(cuopo_inputs *in);
  * evaluated in float exactly as the reference does. */
 cuopo_status cuopo_derive_params(const cuopo_inputs *in, cuopo_params *out, cuopo_info *info);
 
+/* The same derivation for `count` instances at once on the device (the
+ * batched set-up of a sweep): one warp per instance runs the temperature
+ * scan, then the derivation, from the same source as cuopo_derive_params.
+ * in_dev, out_dev and status_dev (CUOPO_OK or CUOPO_EINVAL per instance)
+ * are device arrays; no cuopo_info.  Float operations round as on the host;
+ * CUDA's powf/pow may differ from glibc's in the last bits, so the result
+ * can differ from the host's (which is bit-exact with the reference's) by a
+ * few float ulps.  Asynchronous on stream. */
+cuopo_status cuopo_derive_params_device(const cuopo_inputs *in_dev, int count, cuopo_params *out_dev,
+                                        int *status_dev, void *stream);
+
 /* Sellmeier model of the crystal: which = 0 n, 1 dn/dl, 2 d2n/dl2, 3 d3n/dl3,
  * 4 group velocity, 5 GVD, 6 TOD.  L in um, T in C.  (ppln.cuh:33-189) */
 float cuopo_sellmeier(int crystal, int which, float L, float T);
