@@ -472,6 +472,20 @@ def run_cuopo(args):
 
     # per-grid-size kernel timing (untimed for `value`): each grid size's instances of the sweep alone
     per_size = time_per_size(cu, base, insts_o, peak, stream) if rank == 0 else None
+    fp64 = None
+    if rank == 0 and per_size:
+        # the FP64 solver on the same per-size batches, and the sweep rate it implies (same round trips)
+        per64 = time_per_size(cu, base, insts_o, peak, stream, precision=cu.F64)
+        t64 = 0.0
+        for n in per64:
+            rts_n = float(np.sum(rts[nt_o == int(n)]))
+            t64 += rts_n * per64[n]["ms"] * 1e-3 / (per64[n]["round_trips"] * per64[n]["instances"])
+        fp64 = {"per_size": {n: {k: v for k, v in d.items() if k in ("kernel", "ms", "tflops")}
+                             for n, d in per64.items()},
+                "sweep_solves_per_s_estimate": len(insts_o) / t64 if t64 > 0 else None,
+                "note": "FP64 fields and arithmetic (the FP64 plan kernels, FP64 rate counted against the same "
+                        "algorithmic work); the sweep estimate scales each grid size's per-instance round-trip "
+                        "time by the FP32 sweep's round trips (one grid size at a time, no overlap of sizes)"}
 
     validation = None
     if not args.no_validate and rank == 0:
@@ -534,6 +548,7 @@ def run_cuopo(args):
                                "traffic_per": "step (one launch per grid size; ncu-measured bytes per instance-point)",
                                "kernel": "ssfm_kernel (fused round trips, all grid sizes at once)"},
             "per_size": per_size,
+            "fp64_solver": fp64,
             "cpu_baseline": cpu,
             "e2e": {"value": done_all / (e2e_ms * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(total * 8 / K), "d2h_bytes_per_step": int((total * 8 + len(insts) * 16) / K)},
@@ -551,20 +566,25 @@ def run_cuopo(args):
     return 0
 
 
-def time_per_size(cu, base, insts_o, peak, stream, n_rt: int = 20) -> dict:
+def time_per_size(cu, base, insts_o, peak, stream, n_rt: int = 20, precision=None) -> dict:
     """Each grid size's kernel alone: a batch of that size's sweep instances
     runs n_rt round trips from noise (one launch) between CUDA events on the
-    launching stream; algorithmic TFLOP/s and fraction of the FP32 probe."""
+    launching stream; algorithmic TFLOP/s and fraction of the FP32 probe
+    (with precision F64: the FP64 solver's kernels, same work counted)."""
     import torch
+    prec = cu.F32 if precision is None else precision
     rate = None
-    if TRAFFIC_RECORD.exists():
+    if TRAFFIC_RECORD.exists() and prec == cu.F32:
         rate = json.loads(TRAFFIC_RECORD.read_text()).get("dram_bytes_per_instance_point")
     out = {}
     for n in sorted(set(int(x["n_t"]) for x in insts_o)):
         sub = [x for x in insts_o if x["n_t"] == n]
-        m, cl = cu.kernel_config(n)
-        with cu.Batch(base, sub) as b:
-            b.seed_noise(NOISE)
+        m, cl = cu.kernel_config(n, precision=prec)
+        with cu.Batch(base, sub, precision=prec) as b:
+            if prec == cu.F32:
+                b.seed_noise(NOISE)
+            else:
+                b.set_signal(np.concatenate([cu.noise_host(n, NOISE, x["seed"]) for x in sub]).astype(np.complex128))
             b.reset()
             b.step(n_rt, n_rt, 0.0, 1)     # warm-up launch
             b.reset()
@@ -669,10 +689,12 @@ def validate_fp64(cu, base, insts_o, h_init, ps, rts, flags, per_class: int = 1)
         p = cu.Params(**base.to_dict())
         p.n_t, p.Rs, p.delta, p.gdd, p.ap0 = x["n_t"], x["Rs"], x["delta"], x["gdd"], x["ap0"]
         plan = cu.Plan(p, precision=cu.F64)
-        st = torch.cuda.Stream()
         As = h_init[offs[k]:offs[k + 1]].to("cuda", torch.complex128)
         Ap = torch.zeros_like(As)
         hist = torch.zeros(int(rts[k]), dtype=torch.float64, device="cuda")
+        # the inputs were made on the current stream: the instance's own stream waits for them
+        st = torch.cuda.Stream()
+        st.wait_stream(torch.cuda.current_stream())
         plan.round_trips(Ap, As, None, None, 0, 0, int(rts[k]), ps_hist=hist, stream=st)
         runs.append((plan, hist))
     torch.cuda.synchronize()

@@ -427,7 +427,7 @@ def _arm(r, count):
     return out
 
 
-def _judge(r, ref):
+def _vs_plain(r, ref):
     both = (ref["flags"] == 1) & (r["flags"] == 1) & (ref["ps"] > 1e-20)
     err = np.abs(r["ps"][both] - ref["ps"][both]) / ref["ps"][both]
     return {"instances": int(np.sum(both)), "max_rel_err_ps": float(np.max(err)) if err.size else None,
@@ -443,7 +443,7 @@ def evaluate(model: WarmStartModel, count: int, seed: int, n_t: int = 8192, n_z:
     else the same noise) and a control without the network (noise seeded
     with sigma `control_noise`, which also skips part of the build-up).  The
     final signal power of every instance that converged in an arm and in the
-    plain solve is judged against the plain solve's."""
+    plain solve is compared with the plain solve's."""
     from . import sweep
     base, insts, table = sweep.random_cw_sweep(count, seed, n_t_choices=(n_t,), n_z=n_z)
     plain = solve_sweep(base, insts, table, None, max_rt, tol)
@@ -454,12 +454,12 @@ def evaluate(model: WarmStartModel, count: int, seed: int, n_t: int = 8192, n_z:
     out = {"count": count, "seed": seed, "n_t": n_t, "max_rt": max_rt, "tol": tol, "check_tol": check_tol,
            "model": model.kind, "plain": _arm(plain, count), "warm": _arm(warm, count),
            "gain_converged_solves_per_s": rate(warm) / rate(plain) if conv_p else None,
-           "warm_judged_by_plain": _judge(warm, plain)}
+           "warm_vs_plain": _vs_plain(warm, plain)}
     if ctrl is not None:
         out["control_noise"] = control_noise
         out["control"] = _arm(ctrl, count)
         out["control_gain_converged_solves_per_s"] = rate(ctrl) / rate(plain) if conv_p else None
-        out["control_judged_by_plain"] = _judge(ctrl, plain)
+        out["control_vs_plain"] = _vs_plain(ctrl, plain)
     return out
 
 
@@ -484,7 +484,9 @@ def main():
     ap.add_argument("--eval-seed", type=int, default=7)
     ap.add_argument("--kind", choices=["band", "low_modes"], default="band")
     ap.add_argument("--save-data", type=str, default="", help="write the generated training set (npz)")
-    ap.add_argument("--data", type=str, default="", help="train on a saved training set instead of solving")
+    ap.add_argument("--data", type=str, default="",
+                    help="comma-separated saved training sets to train on (with --count > 0 a new set is also "
+                         "generated and added)")
     ap.add_argument("--check-tol", type=float, default=0.5)
     ap.add_argument("--out", type=str, default=str(MODEL_PATH))
     ap.add_argument("--summary", type=str, default="")
@@ -505,14 +507,17 @@ def main():
         print(json.dumps({"steps": a.steps, "batch": a.batch, "ms_per_step": ev[0].elapsed_time(ev[1]) / a.steps}))
         return
     if a.cmd == "train":
-        if a.data:
-            z = np.load(a.data)
-            d = {k: z[k] for k in z.files}
-            d["seconds"] = float(d["seconds"])
-        else:
-            d = generate_data(a.count, a.seed, n_t=a.n_t, kind=a.kind)
+        parts = []
+        for path in [q for q in a.data.split(",") if q]:
+            z = np.load(path)
+            parts.append({k: z[k] for k in ("x", "y", "ps", "seconds")})
+        if a.count > 0:
+            g = generate_data(a.count, a.seed, n_t=a.n_t, kind=a.kind)
             if a.save_data:
-                np.savez_compressed(a.save_data, x=d["x"], y=d["y"], ps=d["ps"], seconds=d["seconds"])
+                np.savez_compressed(a.save_data, x=g["x"], y=g["y"], ps=g["ps"], seconds=g["seconds"])
+            parts.append(g)
+        d = {"x": np.concatenate([q["x"] for q in parts]), "y": np.concatenate([q["y"] for q in parts]),
+             "seconds": float(sum(float(q["seconds"]) for q in parts))}
         y = d["y"]
         if a.kind == "band":
             amp = 1.0
@@ -523,11 +528,11 @@ def main():
         t0 = time.perf_counter()
         losses = train(mlp, d["x"], y / amp, a.steps, batch=a.batch, lr=a.lr, seed=a.seed)
         train_s = time.perf_counter() - t0
-        model = WarmStartModel(mlp, amp, {"kind": a.kind, "count": a.count, "converged": int(len(y)),
+        model = WarmStartModel(mlp, amp, {"kind": a.kind, "sets": len(parts), "converged": int(len(y)),
                                           "seed": a.seed, "n_t": a.n_t, "steps": a.steps, "batch": a.batch,
                                           "lr": a.lr, "data_gpu_seconds": round(d["seconds"], 1)})
         model.save(a.out)
-        summary.update(data={"instances": a.count, "converged_states": int(len(y)), "seconds": d["seconds"],
+        summary.update(data={"sets": len(parts), "converged_states": int(len(y)), "seconds": d["seconds"],
                              "n_t": a.n_t},
                        train={"steps": a.steps, "batch": a.batch, "lr": a.lr, "seconds": train_s,
                               "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:]))},

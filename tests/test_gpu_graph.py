@@ -34,6 +34,7 @@ def test_graph_replays_equal_direct_calls(neq, n_t):
         h = torch.zeros(per_block, dtype=torch.float64, device="cuda")
         s = torch.cuda.Stream()
         warm = dev()
+        s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):      # first launch of this kernel outside the capture
             plan.round_trips(warm[0], warm[1], warm[2] if neq == 3 else None, pump, 0, 0, 1, stream=s)
         torch.cuda.synchronize()
