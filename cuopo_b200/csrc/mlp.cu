@@ -1104,6 +1104,7 @@ extern "C" cuopo_status cuopo_gemm_bf16(const void *A, const void *B, float *C, 
                                         int flags, int *err_dev, void *stream)
 {
     if (!A || !B || !C) return cuopo_fail(CUOPO_EINVAL, "gemm_bf16: NULL argument");
+    if ((uintptr_t)C & 15) return cuopo_fail(CUOPO_EINVAL, "gemm_bf16: C must be 16-byte aligned");
     if (M < 128 || M % 128 || N < 64 || N % 64 || K < 64 || K % 64 || split < 1 || (K / 64) % split)
         return cuopo_fail(CUOPO_EINVAL, "gemm_bf16: M multiple of 128, N of 64, K of 64, split dividing K/64");
     const int bn = (N % 128 == 0) ? 128 : 64;

@@ -25,6 +25,7 @@ every run from noise, src/headers/functions.cuh:58-71).
 """
 from __future__ import annotations
 
+import ast
 import ctypes as C
 import time
 from pathlib import Path
@@ -257,7 +258,7 @@ class WarmStartModel:
         p[~bias] = (z["weights_bf16"].astype(np.uint32) << 16).view(np.float32)
         p[bias] = z["biases"]
         mlp.set_params(p)
-        meta = eval(str(z["meta"]), {"__builtins__": {}}) if "meta" in z else {}
+        meta = ast.literal_eval(str(z["meta"])) if "meta" in z else {}
         return WarmStartModel(mlp, float(z["amp_scale"]), meta)
 
     def predict_modes(self, feats):

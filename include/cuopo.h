@@ -381,7 +381,8 @@ cuopo_status cuopo_crystal_pass_noalloc(const cuopo_params *p, const float *w_ho
  * all outputs.  Limits: 1 <= n_in <= 64, width and n_out multiples of 128
  * (n_out <= 1024), 1 <= depth <= 10.  Device buffers are sized for
  * max_batch rows (rounded up to 128).  Weights start uniform in
- * +-sqrt(6 / fan_in) from `seed`, biases at zero.
+ * +-sqrt(6 / fan_in) from `seed`, biases at zero.  A network object is
+ * not thread-safe: use it from one host thread (one stream at a time).
  */
 typedef struct cuopo_mlp cuopo_mlp;
 
