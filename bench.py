@@ -696,11 +696,13 @@ def validate_fp64(cu, base, insts_o, h_init, ps, rts, flags, per_class: int = 1)
         st = torch.cuda.Stream()
         st.wait_stream(torch.cuda.current_stream())
         plan.round_trips(Ap, As, None, None, 0, 0, int(rts[k]), ps_hist=hist, stream=st)
-        runs.append((plan, hist))
+        # the fields stay referenced until the streams are done: torch's allocator
+        # does not see the library's use of them on `st`
+        runs.append((plan, hist, As, Ap))
     torch.cuda.synchronize()
-    ps64 = np.array([h[-1].item() for _, h in runs])
-    for plan, _ in runs:
-        plan.close()
+    ps64 = np.array([r[1][-1].item() for r in runs])
+    for r in runs:
+        r[0].close()
     err = np.abs(ps[idx] - ps64) / np.abs(ps64)
     cases = [{"n_t": int(insts_o[k]["n_t"]), "class": "converged" if flags[k] == 1 else "rt_limit",
               "rts": int(rts[k]), "rel_err_ps": float(e)} for k, e in zip(idx, err)]

@@ -131,6 +131,9 @@ SIGNATURES = {
     "cuopo_mlp_gradients": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "cuopo_mlp_train_step": (_i, [_vp, _vp, _vp, _i, C.c_float, _vp, _vp]),
     "cuopo_mlp_status": (_i, [_vp]),
+    "cuopo_mlp_grad_step": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
+    "cuopo_mlp_grad_buffer": (_i, [_vp, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_long)]),
+    "cuopo_mlp_apply_adam": (_i, [_vp, C.c_float, C.c_float, _vp]),
     "cuopo_gemm_bf16": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp]),
     "cuopo_fields_from_modes": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
     "cuopo_modes_from_spectrum": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),

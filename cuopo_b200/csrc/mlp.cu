@@ -604,6 +604,7 @@ struct AdamArgs {
     float *p, *g, *m, *v;
     const float *adam;  /* [lr, 1 - beta1^t, 1 - beta2^t] */
     float beta1, beta2, eps;
+    float gscale;       /* the gradient is multiplied by this (1 / ranks after a sum over ranks) */
     int update;         /* 0: only refresh the BF16 copies */
     int nseg;
     Seg seg[MAX_SEG];
@@ -615,7 +616,7 @@ __global__ void adam_kernel(const AdamArgs a, long total)
     if (i >= total) return;
     float p = a.p[i];
     if (a.update) {
-        const float g = a.g[i];
+        const float g = a.g[i] * a.gscale;
         const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
         const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
         a.m[i] = m;
@@ -665,9 +666,12 @@ struct cuopo_mlp {
     std::vector<CUtensorMap> mA_fwd, mB_fwd, mA_dW, mB_dW, mA_dX, mB_dX;
     std::vector<void *> allocs;
     AdamArgs adam_args;
-    cudaGraphExec_t graph;
+    cudaGraphExec_t graph;        /* forward, loss, backward, Adam */
     int graph_batch;
     cudaStream_t graph_stream;
+    cudaGraphExec_t grad_graph;   /* forward, loss, backward (data-parallel steps) */
+    int grad_graph_batch;
+    cudaStream_t grad_graph_stream;
 };
 
 namespace {
@@ -755,10 +759,11 @@ cuopo_status backward(cuopo_mlp *m, int batch, int rows_used, cudaStream_t st)
     return CUOPO_OK;
 }
 
-cuopo_status run_adam(cuopo_mlp *m, int update, cudaStream_t st)
+cuopo_status run_adam(cuopo_mlp *m, int update, cudaStream_t st, float gscale = 1.0f)
 {
     AdamArgs a = m->adam_args;
     a.update = update;
+    a.gscale = gscale;
     const int tpb = 256;
     adam_kernel<<<(unsigned)((m->P + tpb - 1) / tpb), tpb, 0, st>>>(a, m->P);
     cuopo_status s = launch_check(cudaGetLastError(), "mlp: adam kernel");
@@ -836,6 +841,9 @@ extern "C" cuopo_status cuopo_mlp_create(cuopo_mlp **out, int n_in, int width, i
     m->graph = nullptr;
     m->graph_batch = -1;
     m->graph_stream = nullptr;
+    m->grad_graph = nullptr;
+    m->grad_graph_batch = -1;
+    m->grad_graph_stream = nullptr;
     long off = 0;
     for (int l = 0; l < m->L; l++) {
         m->N.push_back(l == m->L - 1 ? n_out : width);
@@ -912,6 +920,7 @@ extern "C" cuopo_status cuopo_mlp_create(cuopo_mlp **out, int n_in, int width, i
     a.beta1 = 0.9f;
     a.beta2 = 0.999f;
     a.eps = 1e-8f;
+    a.gscale = 1.0f;
     a.nseg = 2 * m->L;
     for (int l = 0; l < m->L; l++) {
         a.seg[2 * l] = Seg{m->w_off[l], (long)m->N[l] * m->Kp[l], m->N[l], m->Kp[l], m->w_bf[l], m->wT_bf[l]};
@@ -946,6 +955,7 @@ extern "C" cuopo_status cuopo_mlp_destroy(cuopo_mlp *m)
 {
     if (!m) return CUOPO_OK;
     if (m->graph) cudaGraphExecDestroy(m->graph);
+    if (m->grad_graph) cudaGraphExecDestroy(m->grad_graph);
     for (void *p : m->allocs) cudaFree(p);
     delete m;
     return CUOPO_OK;
@@ -1040,6 +1050,58 @@ extern "C" cuopo_status cuopo_mlp_gradients(cuopo_mlp *m, const float *x, const 
     return CUOPO_OK;
 }
 
+namespace {
+
+/* Captures forward + loss + backward (+ Adam) for one batch size on a
+ * stream into *exec (replacing an earlier graph). */
+cuopo_status capture_step(cuopo_mlp *m, int batch, int rows, cudaStream_t st, bool with_adam, cudaGraphExec_t *exec)
+{
+    if (*exec) {
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+    }
+    cudaError_t e;
+    cudaStream_t cap = st;
+    bool own = false;
+    if (!cap) {
+        if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_err(e, "mlp: capture stream");
+        own = true;
+        if ((e = cudaStreamSynchronize(0)) != cudaSuccess) {
+            cudaStreamDestroy(cap);
+            return cuda_err(e, "mlp: capture");
+        }
+    }
+    cudaGraph_t g = nullptr;
+    if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        if (own) cudaStreamDestroy(cap);
+        return cuda_err(e, "mlp: begin capture");
+    }
+    cuopo_status s = forward(m, rows, true, cap);
+    if (s == CUOPO_OK) s = backward(m, batch, rows, cap);
+    if (s == CUOPO_OK && with_adam) s = run_adam(m, 1, cap);
+    e = cudaStreamEndCapture(cap, &g);
+    if (s == CUOPO_OK && e != cudaSuccess) s = cuda_err(e, "mlp: end capture");
+    if (s == CUOPO_OK) {
+        e = cudaGraphInstantiate(exec, g, 0);
+        if (e != cudaSuccess) s = cuda_err(e, "mlp: instantiate");
+    }
+    if (g) cudaGraphDestroy(g);
+    if (own) cudaStreamDestroy(cap);
+    return s;
+}
+
+/* Step counter and Adam scalars for a standalone update. */
+__global__ void adam_scalars_kernel(int *step, float *adam, float lr, float beta1, float beta2)
+{
+    const int t = ++*step;
+    adam[0] = lr;
+    adam[1] = 1.0f - powf(beta1, (float)t);
+    adam[2] = 1.0f - powf(beta2, (float)t);
+}
+
+}  /* namespace */
+
 extern "C" cuopo_status cuopo_mlp_train_step(cuopo_mlp *m, const float *x, const float *t, int batch, float lr,
                                              float *loss, void *stream)
 {
@@ -1051,44 +1113,57 @@ extern "C" cuopo_status cuopo_mlp_train_step(cuopo_mlp *m, const float *x, const
     /* the step's inputs go into the network's own buffers outside the graph */
     cuopo_status s = pack(m, x, t, batch, rows, true, lr, st);
     if (s != CUOPO_OK) return s;
-    cudaError_t e;
     if (!m->graph || m->graph_batch != batch || m->graph_stream != st) {
-        if (m->graph) {
-            cudaGraphExecDestroy(m->graph);
-            m->graph = nullptr;
-        }
-        /* capture forward + loss + backward + Adam once per (batch, stream) */
-        cudaStream_t cap = st;
-        bool own = false;
-        if (!cap) {
-            if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess)
-                return cuda_err(e, "mlp_train_step: stream");
-            own = true;
-            if ((e = cudaStreamSynchronize(0)) != cudaSuccess) return cuda_err(e, "mlp_train_step");
-        }
-        cudaGraph_t g = nullptr;
-        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
-            return cuda_err(e, "mlp_train_step: begin capture");
-        s = forward(m, rows, true, cap);
-        if (s == CUOPO_OK) s = backward(m, batch, rows, cap);
-        if (s == CUOPO_OK) s = run_adam(m, 1, cap);
-        e = cudaStreamEndCapture(cap, &g);
-        if (s != CUOPO_OK) {
-            if (g) cudaGraphDestroy(g);
-            return s;
-        }
-        if (e != cudaSuccess) return cuda_err(e, "mlp_train_step: end capture");
-        e = cudaGraphInstantiate(&m->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (own) cudaStreamDestroy(cap);
-        if (e != cudaSuccess) return cuda_err(e, "mlp_train_step: instantiate");
+        /* forward + loss + backward + Adam, captured once per (batch, stream) */
+        if ((s = capture_step(m, batch, rows, st, true, &m->graph)) != CUOPO_OK) return s;
         m->graph_batch = batch;
         m->graph_stream = st;
     }
+    cudaError_t e;
     if ((e = cudaGraphLaunch(m->graph, st)) != cudaSuccess) return cuda_err(e, "mlp_train_step: graph launch");
     if (loss && (e = cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
         return cuda_err(e, "mlp_train_step: loss");
     return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_mlp_grad_step(cuopo_mlp *m, const float *x, const float *t, int batch, float *loss,
+                                            void *stream)
+{
+    if (!m || !x || !t) return cuopo_fail(CUOPO_EINVAL, "mlp_grad_step: NULL argument");
+    if (batch < 1 || batch > m->max_batch) return cuopo_fail(CUOPO_EINVAL, "mlp_grad_step: batch outside [1, max_batch]");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rows = round128(batch);
+    cuopo_status s = pack(m, x, t, batch, rows, true, 0.f, st);
+    if (s != CUOPO_OK) return s;
+    if (!m->grad_graph || m->grad_graph_batch != batch || m->grad_graph_stream != st) {
+        if ((s = capture_step(m, batch, rows, st, false, &m->grad_graph)) != CUOPO_OK) return s;
+        m->grad_graph_batch = batch;
+        m->grad_graph_stream = st;
+    }
+    cudaError_t e;
+    if ((e = cudaGraphLaunch(m->grad_graph, st)) != cudaSuccess) return cuda_err(e, "mlp_grad_step: graph launch");
+    if (loss && (e = cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+        return cuda_err(e, "mlp_grad_step: loss");
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_mlp_grad_buffer(cuopo_mlp *m, float **grad_dev, long *count)
+{
+    if (!m || !grad_dev || !count) return cuopo_fail(CUOPO_EINVAL, "mlp_grad_buffer: NULL argument");
+    *grad_dev = m->grads;
+    *count = m->P;
+    return CUOPO_OK;
+}
+
+extern "C" cuopo_status cuopo_mlp_apply_adam(cuopo_mlp *m, float lr, float grad_scale, void *stream)
+{
+    if (!m) return cuopo_fail(CUOPO_EINVAL, "mlp_apply_adam: NULL argument");
+    if (!(lr > 0) || !(grad_scale > 0)) return cuopo_fail(CUOPO_EINVAL, "mlp_apply_adam: lr and grad_scale must be > 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    adam_scalars_kernel<<<1, 1, 0, st>>>(m->step, m->adam, lr, 0.9f, 0.999f);
+    cuopo_status s = launch_check(cudaGetLastError(), "mlp_apply_adam: scalars");
+    if (s != CUOPO_OK) return s;
+    return run_adam(m, 1, st, grad_scale);
 }
 
 extern "C" cuopo_status cuopo_mlp_status(cuopo_mlp *m)

@@ -123,6 +123,27 @@ class MLP:
     def status(self) -> None:
         check(self._lib.cuopo_mlp_status(self._h))
 
+    def grad_step(self, x, t, loss=None, stream=None) -> None:
+        """Forward, loss and backward on the batch into the network's gradient buffer (asynchronous)."""
+        check(self._lib.cuopo_mlp_grad_step(self._h, x.data_ptr(), t.data_ptr(), x.shape[0],
+                                            None if loss is None else loss.data_ptr(), _stream(stream)))
+
+    def grad_tensor(self):
+        """The network's device gradient buffer as a CUDA float32 tensor (a view, no copy)."""
+        torch = _torch()
+        ptr = C.POINTER(C.c_float)()
+        n = C.c_long()
+        check(self._lib.cuopo_mlp_grad_buffer(self._h, C.byref(ptr), C.byref(n)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n.value,), "typestr": "<f4",
+                                        "data": (C.cast(ptr, C.c_void_p).value, False), "version": 2}
+        return torch.as_tensor(_View(), device="cuda")
+
+    def apply_adam(self, lr: float, grad_scale: float = 1.0, stream=None) -> None:
+        """One Adam step from the gradient buffer times grad_scale (asynchronous)."""
+        check(self._lib.cuopo_mlp_apply_adam(self._h, float(lr), float(grad_scale), _stream(stream)))
+
 
 def gemm_bf16(A, B, split: int = 1, err=None, flags: int = 0, out=None, stream=None):
     """C = A B^T on the tensor cores (A [M][K], B [N][K] CUDA bfloat16) -> float32 [M][N]."""
@@ -339,6 +360,42 @@ def train(mlp: MLP, x: np.ndarray, y: np.ndarray, steps: int, batch: int = 4096,
     mlp.status()
     out = losses.cpu().numpy()
     return out if not log_every else out[::log_every]
+
+
+def train_data_parallel(mlp, x: np.ndarray, y: np.ndarray, steps: int, batch: int = 4096, lr: float = 1e-3,
+                        seed: int = 0, group=None):
+    """Data-parallel Adam over the ranks of torch.distributed (one network
+    copy per rank, NCCL on GPUs): rank r keeps the training rows r, r + W,
+    ... and draws its minibatches from them; every step runs forward and
+    backward on the rank's batch, sums the gradient buffers over the ranks
+    (all-reduce on the current stream) and applies one Adam step with the
+    mean.  `mlp` is any object with grad_step / grad_tensor / apply_adam
+    (the MLP above).  Without an initialised process group it runs on one
+    rank.  Returns this rank's per-step losses."""
+    torch = _torch()
+    import torch.distributed as dist
+    on = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size(group) if on else 1
+    rank = dist.get_rank(group) if on else 0
+    dev = mlp.grad_tensor().device
+    X = torch.from_numpy(np.ascontiguousarray(x[rank::world], np.float32)).to(dev)
+    Y = torch.from_numpy(np.ascontiguousarray(y[rank::world], np.float32)).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 7919 * rank)
+    n = X.shape[0]
+    b = n if batch <= 0 or batch >= n else batch
+    losses = torch.zeros(max(1, steps), dtype=torch.float32, device=dev)
+    for s in range(steps):
+        if b == n:
+            xb, yb = X, Y
+        else:
+            idx = torch.randint(0, n, (b,), generator=g, device=dev)
+            xb, yb = X.index_select(0, idx), Y.index_select(0, idx)
+        mlp.grad_step(xb, yb, loss=losses[s])
+        if world > 1:
+            dist.all_reduce(mlp.grad_tensor(), op=dist.ReduceOp.SUM, group=group)
+        mlp.apply_adam(lr if s < 0.7 * steps else 0.1 * lr, grad_scale=1.0 / world)
+    return losses.cpu().numpy()
 
 
 # ------------------------------------------------------------ warm-started solve

@@ -409,6 +409,18 @@ cuopo_status cuopo_mlp_gradients(cuopo_mlp *mlp, const float *x, const float *t,
  * before the update, or NULL.  Asynchronous. */
 cuopo_status cuopo_mlp_train_step(cuopo_mlp *mlp, const float *x, const float *t, int batch, float lr, float *loss,
                                   void *stream);
+/* Data-parallel training over ranks (one network copy per GPU):
+ * grad_step runs forward, loss and backward on the rank's batch (one CUDA
+ * graph per batch size and stream) and leaves the gradient in the network's
+ * own device buffer, which grad_buffer exposes (FP32, `count` values, an
+ * internal layout that an element-wise sum over ranks -- an NCCL
+ * all-reduce -- keeps valid); apply_adam then takes one Adam step from that
+ * buffer multiplied by grad_scale (1 / ranks after a sum).  With the same
+ * parameters on every rank and equal batches, the ranks stay identical. */
+cuopo_status cuopo_mlp_grad_step(cuopo_mlp *mlp, const float *x, const float *t, int batch, float *loss,
+                                 void *stream);
+cuopo_status cuopo_mlp_grad_buffer(cuopo_mlp *mlp, float **grad_dev, long *count);
+cuopo_status cuopo_mlp_apply_adam(cuopo_mlp *mlp, float lr, float grad_scale, void *stream);
 /* Waits for the device and reports CUOPO_ETIMEOUT if a GEMM's bounded wait
  * gave up since the last check. */
 cuopo_status cuopo_mlp_status(cuopo_mlp *mlp);

@@ -208,3 +208,29 @@ def test_band_targets_and_synthesis_round_trip():
     assert _rel(got, want) < 1e-4
     pairs = c[(q0 + k) % n_t] * c[(-q0 - k) % n_t]
     assert abs(np.angle(pairs.sum()) - phi) < 1e-4
+
+
+def test_grad_step_and_adam_equal_train_step():
+    """The data-parallel pieces (cuopo_mlp_grad_step, the gradient buffer,
+    cuopo_mlp_apply_adam) take the same steps as cuopo_mlp_train_step on
+    one rank; the gradient buffer is the device view the all-reduce uses."""
+    from cuopo_b200 import warmstart as ws
+    rng = np.random.default_rng(12)
+    x = torch.from_numpy(rng.uniform(-1, 1, (256, 4)).astype(np.float32)).cuda()
+    t = torch.from_numpy((0.5 * rng.standard_normal((256, 128))).astype(np.float32)).cuda()
+    a = ws.MLP(4, 128, 2, 128, max_batch=256, seed=21)
+    b = ws.MLP(4, 128, 2, 128, max_batch=256, seed=21)
+    lr = 1e-3
+    for _ in range(3):
+        a.train_step(x, t, lr)
+        b.grad_step(x, t)
+        g = b.grad_tensor()
+        assert g.is_cuda and g.numel() >= b.n_params
+        g.mul_(2.0)                      # as after a sum over two identical ranks ...
+        b.apply_adam(lr, grad_scale=0.5)  # ... and the mean
+    a.status()
+    b.status()
+    pa, pb = a.get_params(), b.get_params()
+    a.close()
+    b.close()
+    assert np.max(np.abs(pa - pb)) <= 1e-5 * lr * 3 + 1e-6 * np.max(np.abs(pa))
