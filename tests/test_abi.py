@@ -42,3 +42,31 @@ def test_version_and_errors():
         assert "n_eqs" in str(e)
     else:
         raise AssertionError("invalid n_eqs accepted")
+
+
+def test_new_entry_points_reject_bad_arguments_before_touching_the_gpu():
+    """Argument checks of the warm-start and device set-up entry points run
+    before any CUDA call, so they answer CUOPO_EINVAL on a machine without a
+    GPU as well."""
+    import ctypes as C
+    lib = cu.load()
+    h = C.c_void_p()
+    # MLP: n_in > 64, width not a multiple of 128, depth 0
+    assert lib.cuopo_mlp_create(C.byref(h), 65, 512, 4, 512, 4096, 0) == cu.EINVAL
+    assert lib.cuopo_mlp_create(C.byref(h), 4, 500, 4, 512, 4096, 0) == cu.EINVAL
+    assert lib.cuopo_mlp_create(C.byref(h), 4, 512, 0, 512, 4096, 0) == cu.EINVAL
+    assert lib.cuopo_mlp_create(None, 4, 512, 4, 512, 4096, 0) == cu.EINVAL
+    # GEMM: NULL operands, M not a multiple of 128
+    assert lib.cuopo_gemm_bf16(None, None, None, 128, 64, 64, 1, 0, None, None) == cu.EINVAL
+    buf = (C.c_float * 16)()
+    assert lib.cuopo_gemm_bf16(buf, buf, buf, 100, 64, 64, 1, 0, None, None) == cu.EINVAL
+    # field synthesis: n_t not a power of 2 / too small, n_modes not a multiple of 16
+    assert lib.cuopo_fields_from_bands(buf, 1, 100, 1.0, buf, None, None) == cu.EINVAL
+    assert lib.cuopo_fields_from_modes(buf, 1, 20, 1024, 1.0, buf, None) == cu.EINVAL
+    assert lib.cuopo_modes_from_spectrum(buf, 1, 1024, 48, 1.0, buf, None) == cu.EINVAL
+    # device set-up: NULL arrays, no instances
+    assert lib.cuopo_derive_params_device(None, 4, None, None, None) == cu.EINVAL
+    assert lib.cuopo_derive_params_device(buf, 0, buf, buf, None) == cu.EINVAL
+    # data-parallel pieces on a NULL network
+    assert lib.cuopo_mlp_apply_adam(None, 1e-3, 1.0, None) == cu.EINVAL
+    assert lib.cuopo_mlp_grad_buffer(None, None, None) == cu.EINVAL
