@@ -38,6 +38,10 @@ def _inputs(count, seed):
                                 delta=float(rng.uniform(-1, 1)), gdd_percent=float(rng.uniform(-100, 100)),
                                 lcr_mm=float(rng.uniform(2, 30)), use_eom=int(rng.integers(0, 2)),
                                 mod_depth_pi=float(rng.uniform(0.1, 1)), freq_det_mhz=float(rng.uniform(0, 10)))
+        if k % 7 == 0:
+            # the argv[2] temperature instead of the scan
+            inp.temp_from_scan = 0
+            inp.temp_c = float(rng.uniform(20, 120))
         out.append(inp)
     return out
 

@@ -26,7 +26,7 @@ torch = pytest.importorskip("torch")
 
 
 def dev(x, prec):
-    dt = torch.complex64 if prec == cu.F32 else torch.complex128
+    dt = torch.complex128 if prec == cu.F64 else torch.complex64
     return torch.from_numpy(np.ascontiguousarray(x)).to("cuda", dt)
 
 
@@ -91,6 +91,21 @@ def test_pass_f32_vs_oracle(neq, n_t):
     ref = run_pass_oracle(p, Ap.astype(np.complex64).astype(np.complex128),
                           As.astype(np.complex64).astype(np.complex128),
                           None if Ai is None else Ai.astype(np.complex64).astype(np.complex128))
+    for g, r in zip(got, ref):
+        if r is not None:
+            assert rel_l2(g, r) < 5e-6
+
+
+@pytest.mark.parametrize("neq,n_t", [(2, 1024), (2, 8192), (2, 32768), (3, 4096), (3, 65536)])
+def test_pass_phase32_vs_oracle(neq, n_t):
+    """CUOPO_F32_PHASE32 plans (phase factors from FP32 sin/cos after FP64
+    argument reduction) against the FP64 oracle: the same bound per pass as
+    the FP32 plans with FP64-formed phases, 5e-6 relative L2."""
+    p = make_params(neq, n_t, n_z=6)
+    Ap, As, Ai = fields(p, 40 + n_t)
+    c = (lambda a: None if a is None else a.astype(np.complex64))
+    got = run_pass_gpu(p, cu.F32_PHASE32, c(Ap), c(As), c(Ai))
+    ref = run_pass_oracle(p, *[None if a is None else a.astype(np.complex128) for a in (c(Ap), c(As), c(Ai))])
     for g, r in zip(got, ref):
         if r is not None:
             assert rel_l2(g, r) < 5e-6
