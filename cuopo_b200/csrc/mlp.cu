@@ -37,6 +37,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "cuopo.h"
@@ -145,6 +146,12 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
+
+/* Programmatic dependent launch: wait for the previous kernel in the stream
+ * (a no-op when this grid was launched without the attribute), and let the
+ * next one start its prologue early. */
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -350,6 +357,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *slot;
+    /* everything above is this CTA's own set-up; the operands and the
+     * epilogue's inputs come from the previous kernel */
+    griddep_wait();
+    griddep_launch();
 
     __shared__ int s_err;
     if (threadIdx.x == 0) s_err = 0;
@@ -442,6 +453,30 @@ cuopo_status encode_bf16(CUtensorMap *m, const void *base, long rows, long cols,
 
 cudaError_t prepare_gemm();
 
+/* Set while a training step is being captured: its kernels are launched with
+ * programmatic stream serialization, so each one's launch and set-up overlap
+ * the previous one's tail (every kernel waits with griddepcontrol.wait
+ * before it reads the previous one's results). */
+thread_local int g_pdl = 0; /* 0 off; 1 on from the next launch on; 2 on */
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args)
+{
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl == 2 ? 1 : 0;
+    if (g_pdl) g_pdl = 2;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int BN>
 cudaError_t launch_gemm_bn(const CUtensorMap &a, const CUtensorMap &b, const Epi &ep, int M, int N, int K, int split,
                            cudaStream_t st)
@@ -449,8 +484,9 @@ cudaError_t launch_gemm_bn(const CUtensorMap &a, const CUtensorMap &b, const Epi
     cudaError_t attr = prepare_gemm();
     if (attr != cudaSuccess) return attr;
     dim3 grid((unsigned)(M / BM), (unsigned)(N / BN), (unsigned)split);
-    tc_gemm_kernel<BN><<<grid, NTHREADS, gemm_smem_bytes<BN>(), st>>>(a, b, ep, (K / BK) / split);
-    return cudaGetLastError();
+    cudaError_t e = launch_k(tc_gemm_kernel<BN>, grid, dim3(NTHREADS), gemm_smem_bytes<BN>(), st, a, b, ep,
+                             (K / BK) / split);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 /* C = A B^T with tile width bn (64 or 128); K split into `split` slices. */
@@ -553,6 +589,8 @@ constexpr int MSE_ROWS = 16;
 __global__ void mse_kernel(const float *y, const float *tgt, bf16 *g, bf16 *gT, float *db, float *loss, int batch,
                            int n_out, int ldt)
 {
+    griddep_wait();
+    griddep_launch();
     const int j = threadIdx.x, r0 = blockIdx.x * MSE_ROWS;
     const float scale = 2.0f / ((float)batch * (float)n_out);
     float csum = 0.f, lsum = 0.f;
@@ -612,6 +650,8 @@ struct AdamArgs {
 
 __global__ void adam_kernel(const AdamArgs a, long total)
 {
+    griddep_wait();
+    griddep_launch();
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     float p = a.p[i];
@@ -636,6 +676,8 @@ __global__ void adam_kernel(const AdamArgs a, long total)
  * segment (a.seg[2 l]). */
 __global__ void transpose_weights_kernel(const AdamArgs a)
 {
+    griddep_wait();
+    griddep_launch();
     __shared__ bf16 tile[32][33];
     const Seg &sg = a.seg[2 * blockIdx.z];
     const int n0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
@@ -721,16 +763,28 @@ cuopo_status forward(cuopo_mlp *m, int rows_used, bool train, cudaStream_t st)
     return CUOPO_OK;
 }
 
-/* Loss, gradients (into m->grads, zeroed here) over rows_used rows. */
-cuopo_status backward(cuopo_mlp *m, int batch, int rows_used, cudaStream_t st)
+cuopo_status zero_grads(cuopo_mlp *m, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(m->grads, 0, sizeof(float) * m->P, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->loss, 0, sizeof(float), st);
-    if (e != cudaSuccess) return cuda_err(e, "mlp: memset");
+    return e != cudaSuccess ? cuda_err(e, "mlp: memset") : CUOPO_OK;
+}
+
+/* Loss, gradients (into m->grads) over rows_used rows; `zero`: clear the
+ * gradient and loss accumulators first (a captured step clears them before
+ * its forward pass, so that its kernels follow one another directly). */
+cuopo_status backward(cuopo_mlp *m, int batch, int rows_used, cudaStream_t st, bool zero = true)
+{
+    cudaError_t e;
+    if (zero) {
+        cuopo_status z = zero_grads(m, st);
+        if (z != CUOPO_OK) return z;
+    }
     const int Lo = m->L - 1;
-    mse_kernel<<<rows_used / MSE_ROWS, m->n_out, 0, st>>>(m->y, m->tgt, m->g_out, m->g_outT, m->grads + m->b_off[Lo],
-                                                   m->loss, batch, m->n_out, m->rows);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "mlp: loss kernel");
+    e = launch_k(mse_kernel, dim3((unsigned)(rows_used / MSE_ROWS)), dim3((unsigned)m->n_out), 0, st,
+                 (const float *)m->y, (const float *)m->tgt, m->g_out, m->g_outT, m->grads + m->b_off[Lo], m->loss,
+                 batch, m->n_out, m->rows);
+    if (e != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return cuda_err(e, "mlp: loss kernel");
     for (int l = Lo; l >= 0; l--) {
         /* dW_l = g_l^T act_{l-1}: M = N_l, N = Kp_l, K = rows_used */
         Epi ew = epi_none(m->Kp[l], m->err);
@@ -765,17 +819,17 @@ cuopo_status run_adam(cuopo_mlp *m, int update, cudaStream_t st, float gscale = 
     a.update = update;
     a.gscale = gscale;
     const int tpb = 256;
-    adam_kernel<<<(unsigned)((m->P + tpb - 1) / tpb), tpb, 0, st>>>(a, m->P);
-    cuopo_status s = launch_check(cudaGetLastError(), "mlp: adam kernel");
+    cudaError_t e = launch_k(adam_kernel, dim3((unsigned)((m->P + tpb - 1) / tpb)), dim3(tpb), 0, st, a, m->P);
+    cuopo_status s = launch_check(e != cudaSuccess ? e : cudaGetLastError(), "mlp: adam kernel");
     if (s != CUOPO_OK) return s;
     int maxN = 0, maxK = 0;
     for (int l = 0; l < m->L; l++) {
         maxN = m->N[l] > maxN ? m->N[l] : maxN;
         maxK = m->Kp[l] > maxK ? m->Kp[l] : maxK;
     }
-    transpose_weights_kernel<<<dim3((unsigned)(maxK / 32), (unsigned)(maxN / 32), (unsigned)m->L), dim3(32, 8), 0,
-                               st>>>(a);
-    return launch_check(cudaGetLastError(), "mlp: weight transpose kernel");
+    e = launch_k(transpose_weights_kernel, dim3((unsigned)(maxK / 32), (unsigned)(maxN / 32), (unsigned)m->L),
+                 dim3(32, 8), 0, st, a);
+    return launch_check(e != cudaSuccess ? e : cudaGetLastError(), "mlp: weight transpose kernel");
 }
 
 cuopo_status pack(cuopo_mlp *m, const float *x, const float *t, int batch, int rows_used, bool train, float lr,
@@ -1077,9 +1131,12 @@ cuopo_status capture_step(cuopo_mlp *m, int batch, int rows, cudaStream_t st, bo
         if (own) cudaStreamDestroy(cap);
         return cuda_err(e, "mlp: begin capture");
     }
-    cuopo_status s = forward(m, rows, true, cap);
-    if (s == CUOPO_OK) s = backward(m, batch, rows, cap);
+    cuopo_status s = zero_grads(m, cap);
+    g_pdl = 1;
+    if (s == CUOPO_OK) s = forward(m, rows, true, cap);
+    if (s == CUOPO_OK) s = backward(m, batch, rows, cap, false);
     if (s == CUOPO_OK && with_adam) s = run_adam(m, 1, cap);
+    g_pdl = 0;
     e = cudaStreamEndCapture(cap, &g);
     if (s == CUOPO_OK && e != cudaSuccess) s = cuda_err(e, "mlp: end capture");
     if (s == CUOPO_OK) {
