@@ -235,12 +235,15 @@ def test_noise_device_matches_host():
 
 # ----------------------------------------------------- vs the reference build
 
-# grids of one CTA (1024, 8192) and of the 4- and 8-CTA cluster kernels the sweep runs (16384, 32768)
+# grids of one CTA (1024, 8192), of the 4- and 8-CTA cluster kernels the sweep runs (16384, 32768) and
+# of the 16-CTA 3-wave kernels of the nanosecond configurations (65536, 131072)
 REF_CASES = [(2, "ppln", 1024, cu.CW, dict(delta=0.05, gdd_percent=50.0, use_eom=1)),
              (2, "ppln", 8192, cu.CW, dict()),
              (2, "ppln", 16384, cu.CW, dict(delta=-0.3, gdd_percent=20.0)),
              (2, "ppln", 32768, cu.CW, dict(delta=0.4)),
-             (3, "spplt", 1024, cu.NS, dict(gdd_percent=30.0))]
+             (3, "spplt", 1024, cu.NS, dict(gdd_percent=30.0)),
+             (3, "spplt", 65536, cu.NS, dict(gdd_percent=20.0)),
+             (3, "spplt", 131072, cu.NS, dict(delta=0.2))]
 
 
 @pytest.mark.parametrize("neq,crystal,n_t,regime,kw", REF_CASES)
