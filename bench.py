@@ -475,13 +475,16 @@ def run_cuopo(args):
     fp64 = None
     if rank == 0 and per_size:
         # the FP64 solver on the same per-size batches, and the sweep rate it implies (same round trips)
-        per64 = time_per_size(cu, base, insts_o, peak, stream, precision=cu.F64)
+        peak64 = cu.probe_fp64_peak()
+        per64 = time_per_size(cu, base, insts_o, peak64, stream, precision=cu.F64)
         t64 = 0.0
         for n in per64:
             rts_n = float(np.sum(rts[nt_o == int(n)]))
             t64 += rts_n * per64[n]["ms"] * 1e-3 / (per64[n]["round_trips"] * per64[n]["instances"])
-        fp64 = {"per_size": {n: {k: v for k, v in d.items() if k in ("kernel", "ms", "tflops")}
+        fp64 = {"per_size": {n: {k: v for k, v in d.items() if k in ("kernel", "ms", "tflops", "frac")}
                              for n, d in per64.items()},
+                "fp64_peak_tflops": peak64,
+                "peak_source": "measured live: fma.rn.f64-chain probe over every SM (cuopo_probe_fp64_peak)",
                 "sweep_solves_per_s_estimate": len(insts_o) / t64 if t64 > 0 else None,
                 "note": "FP64 fields and arithmetic (the FP64 plan kernels, FP64 rate counted against the same "
                         "algorithmic work); the sweep estimate scales each grid size's per-instance round-trip "
@@ -569,8 +572,9 @@ def run_cuopo(args):
 def time_per_size(cu, base, insts_o, peak, stream, n_rt: int = 20, precision=None) -> dict:
     """Each grid size's kernel alone: a batch of that size's sweep instances
     runs n_rt round trips from noise (one launch) between CUDA events on the
-    launching stream; algorithmic TFLOP/s and fraction of the FP32 probe
-    (with precision F64: the FP64 solver's kernels, same work counted)."""
+    launching stream; algorithmic TFLOP/s and fraction of `peak` (the FP32
+    probe; with precision F64 the FP64 solver's kernels, same work counted,
+    against the FP64 probe)."""
     import torch
     prec = cu.F32 if precision is None else precision
     rate = None

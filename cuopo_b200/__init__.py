@@ -9,12 +9,12 @@ from ._lib import (CW, EINVAL, ENOMEM, ENONFINITE, EUNSUPPORTED, F32, F32_PHASE3
 from .api import (Batch, Plan, autotune, autotune_reset, default_inputs, derive_params, derive_params_device, fft_c2c, kernel_config, kernel_select,
                   linspace,
                   make_grids, noise_device, noise_host,
-                  phase_matching_temp, probe_fp32_peak, pump_cw, pump_ns, read_dat_complex, sellmeier, sync, write_dat_complex,
+                  phase_matching_temp, probe_fp32_peak, probe_fp64_peak, pump_cw, pump_ns, read_dat_complex, sellmeier, sync, write_dat_complex,
                   write_dat_real)
 
 __all__ = [
     "CW", "NS", "PPLN", "SPPLT", "F32", "F32_PHASE32", "F64", "OK", "EINVAL", "ENOMEM", "ENONFINITE", "EUNSUPPORTED",
     "Batch", "CuopoError", "autotune", "autotune_reset", "kernel_config", "kernel_select", "Info", "Inputs", "Params", "Plan", "default_inputs", "derive_params", "derive_params_device", "fft_c2c", "linspace",
-    "make_grids", "noise_device", "noise_host", "phase_matching_temp", "probe_fp32_peak", "pump_cw", "pump_ns",
+    "make_grids", "noise_device", "noise_host", "phase_matching_temp", "probe_fp32_peak", "probe_fp64_peak", "pump_cw", "pump_ns",
     "read_dat_complex", "sellmeier", "sync", "write_dat_complex", "write_dat_real", "load",
 ]

@@ -117,6 +117,7 @@ SIGNATURES = {
     "cuopo_batch_history": (_i, [_vp, _i, _vp, _i, _vp]),
     "cuopo_batch_wait": (_i, [_vp, _vp]),
     "cuopo_probe_fp32_peak": (_i, [C.POINTER(_d), _vp]),
+    "cuopo_probe_fp64_peak": (_i, [C.POINTER(_d), _vp]),
     "cuopo_crystal_pass_noalloc": (_i, [C.POINTER(Params), _vp, _vp, _vp, _vp, _vp]),
     "cuopo_autotune": (_i, [C.POINTER(Params), _i, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_d)]),
     "cuopo_autotune_reset": (_i, []),

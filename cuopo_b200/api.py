@@ -229,6 +229,13 @@ def probe_fp32_peak(stream=None) -> float:
     return v.value
 
 
+def probe_fp64_peak(stream=None) -> float:
+    """Measured FP64 FMA throughput of the current device [TFLOP/s]."""
+    v = C.c_double()
+    check(load().cuopo_probe_fp64_peak(C.byref(v), _stream(stream)))
+    return v.value
+
+
 def autotune(base: Params, precision: int = F32, count: int = 148, n_rt: int = 2) -> dict:
     """Times every built kernel configuration for base.n_t on `count` copies of
     the CW instance `base` (n_rt round trips each) and makes the fastest the

@@ -1,8 +1,8 @@
 /*
- * probe.cu -- measured FP32 FMA throughput of the device, the denominator of
- * the solver's roofline (the fused SSFM kernels keep every field on chip, so
- * they are bound by FP32 issue and shared-memory bandwidth, not by HBM or
- * the tensor cores).
+ * probe.cu -- measured FP32 (and FP64) FMA throughput of the device, the
+ * denominators of the solver's roofline (the fused SSFM kernels keep every
+ * field on chip, so they are bound by FP32 / FP64 issue and shared-memory
+ * bandwidth, not by HBM or the tensor cores).
  */
 #include <cuda_runtime.h>
 
@@ -58,7 +58,62 @@ __global__ void __launch_bounds__(256) fma2_probe(float *sink, int iters, float 
     if (s == 12345.678f) sink[blockIdx.x] = s;
 }
 
+/* FP64: 8 independent fma.rn.f64 chains per thread (the FP64 solver's
+ * kernels are bound by this pipe). */
+__global__ void __launch_bounds__(256) dfma_probe(double *sink, int iters, double a, double b)
+{
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = (double)(threadIdx.x + k) * 1e-3;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int r = 0; r < 16; r++)
+#pragma unroll
+            for (int k = 0; k < 8; k++) x[k] = fma(x[k], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 12345.678) sink[blockIdx.x] = s;
+}
+
 }  // namespace
+
+extern "C" cuopo_status cuopo_probe_fp64_peak(double *tflops, void *stream)
+{
+    if (!tflops) return cuopo_fail(CUOPO_EINVAL, "probe_fp64_peak: NULL argument");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    double *sink = nullptr;
+    cudaEvent_t e0, e1;
+    cudaError_t e;
+    if ((e = cudaMalloc(&sink, sizeof(double) * 64 * sms)) != cudaSuccess)
+        return cuopo_fail(CUOPO_ECUDA, cudaGetErrorString(e));
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = 8 * sms, threads = 256, iters = 512;
+    dfma_probe<<<blocks, threads, 0, st>>>(sink, 16, 0.999, 1e-4); /* warm-up */
+    double best = 0.0;
+    for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(e0, st);
+        dfma_probe<<<blocks, threads, 0, st>>>(sink, iters, 0.999, 1e-4);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+        if (ms > 0 && flops / (ms * 1e-3) / 1e12 > best) best = flops / (ms * 1e-3) / 1e12;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuopo_fail(CUOPO_ECUDA, cudaGetErrorString(e));
+    *tflops = best;
+    return CUOPO_OK;
+}
 
 extern "C" cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream)
 {

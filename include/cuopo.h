@@ -465,6 +465,10 @@ cuopo_status cuopo_fields_from_bands(const float *pred, int count, int n_t, doub
  * SM); the denominator of the solver's roofline.  Synchronous. */
 cuopo_status cuopo_probe_fp32_peak(double *tflops, void *stream);
 
+/* The same for FP64 (best of 3 launches of an fma.rn.f64-chain kernel over
+ * every SM): the denominator of the FP64 plans' roofline.  Synchronous. */
+cuopo_status cuopo_probe_fp64_peak(double *tflops, void *stream);
+
 /* Blocks until the plan's work on stream has finished; returns the first
  * asynchronous error. */
 cuopo_status cuopo_sync(void *stream);
