@@ -11,6 +11,8 @@ if str(ROOT) not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+    config.addinivalue_line("markers", "gpu_slow: needs a CUDA GPU and minutes of it; run with -m gpu_slow "
+                                       "(not part of -m gpu)")
 
 
 def _has_gpu() -> bool:
@@ -26,5 +28,5 @@ def pytest_collection_modifyitems(config, items):
         return
     skip = pytest.mark.skip(reason="no CUDA GPU in this environment")
     for item in items:
-        if "gpu" in item.keywords:
+        if "gpu" in item.keywords or "gpu_slow" in item.keywords:
             item.add_marker(skip)
