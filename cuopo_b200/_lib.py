@@ -6,7 +6,6 @@ loudly when it is missing: there is no Python or CPU fallback for the solver.
 from __future__ import annotations
 
 import ctypes as C
-import os
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent

@@ -15,8 +15,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import _lib
-from ._lib import CW, F32, F64, NS, OK, PPLN, SPPLT, CuopoError, Info, Inputs, Params, check, load
+from ._lib import F32, F64, OK, CuopoError, Info, Inputs, Params, check, load
 
 
 def default_inputs(**kw) -> Inputs:

@@ -33,7 +33,7 @@ from pathlib import Path
 import numpy as np
 
 from . import api
-from ._lib import F32, check, load
+from ._lib import check, load
 
 N_MODES = 256
 N_FEATURES = 4

@@ -12,7 +12,6 @@ are the oracle's parameter block).
 from __future__ import annotations
 
 import ctypes as C
-import os
 import subprocess
 from pathlib import Path
 

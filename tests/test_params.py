@@ -1,7 +1,6 @@
 """Host set-up parity: the product's Sellmeier models, temperature scan, grids and
 pump windows against the reference's own host functions (src/headers/ppln.cuh,
 spplt.cuh, functions.cuh, compiled unchanged into oracle/_ref).  Bit-exact."""
-import ctypes as C
 
 import numpy as np
 import pytest
