@@ -21,6 +21,20 @@ void cuopo_noise_pair_host(uint64_t seed, uint64_t stream_id, uint64_t i, double
 
 #ifdef __cplusplus
 }
+
+#include <nvtx3/nvToolsExt.h>
+
+namespace cuopo {
+/* A named NVTX range over the enclosing scope: the library's host calls show
+ * up by name on a profiler's timeline; without a tool attached the push and
+ * pop return at once. */
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+}  // namespace cuopo
 #endif
 
 #endif

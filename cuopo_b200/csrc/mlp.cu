@@ -1066,6 +1066,7 @@ extern "C" cuopo_status cuopo_mlp_get_params(cuopo_mlp *m, float *host)
 
 extern "C" cuopo_status cuopo_mlp_forward(cuopo_mlp *m, const float *x, float *y, int batch, void *stream)
 {
+    cuopo::Range range_("cuopo_mlp_forward");
     if (!m || !x || !y) return cuopo_fail(CUOPO_EINVAL, "mlp_forward: NULL argument");
     if (batch < 1 || batch > m->max_batch) return cuopo_fail(CUOPO_EINVAL, "mlp_forward: batch outside [1, max_batch]");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1080,6 +1081,7 @@ extern "C" cuopo_status cuopo_mlp_forward(cuopo_mlp *m, const float *x, float *y
 extern "C" cuopo_status cuopo_mlp_gradients(cuopo_mlp *m, const float *x, const float *t, int batch, float *grad,
                                             float *loss, void *stream)
 {
+    cuopo::Range range_("cuopo_mlp_gradients");
     if (!m || !x || !t) return cuopo_fail(CUOPO_EINVAL, "mlp_gradients: NULL argument");
     if (batch < 1 || batch > m->max_batch) return cuopo_fail(CUOPO_EINVAL, "mlp_gradients: batch outside [1, max_batch]");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1162,6 +1164,7 @@ __global__ void adam_scalars_kernel(int *step, float *adam, float lr, float beta
 extern "C" cuopo_status cuopo_mlp_train_step(cuopo_mlp *m, const float *x, const float *t, int batch, float lr,
                                              float *loss, void *stream)
 {
+    cuopo::Range range_("cuopo_mlp_train_step");
     if (!m || !x || !t) return cuopo_fail(CUOPO_EINVAL, "mlp_train_step: NULL argument");
     if (batch < 1 || batch > m->max_batch) return cuopo_fail(CUOPO_EINVAL, "mlp_train_step: batch outside [1, max_batch]");
     if (!(lr > 0)) return cuopo_fail(CUOPO_EINVAL, "mlp_train_step: lr must be > 0");
@@ -1186,6 +1189,7 @@ extern "C" cuopo_status cuopo_mlp_train_step(cuopo_mlp *m, const float *x, const
 extern "C" cuopo_status cuopo_mlp_grad_step(cuopo_mlp *m, const float *x, const float *t, int batch, float *loss,
                                             void *stream)
 {
+    cuopo::Range range_("cuopo_mlp_grad_step");
     if (!m || !x || !t) return cuopo_fail(CUOPO_EINVAL, "mlp_grad_step: NULL argument");
     if (batch < 1 || batch > m->max_batch) return cuopo_fail(CUOPO_EINVAL, "mlp_grad_step: batch outside [1, max_batch]");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1214,6 +1218,7 @@ extern "C" cuopo_status cuopo_mlp_grad_buffer(cuopo_mlp *m, float **grad_dev, lo
 
 extern "C" cuopo_status cuopo_mlp_apply_adam(cuopo_mlp *m, float lr, float grad_scale, void *stream)
 {
+    cuopo::Range range_("cuopo_mlp_apply_adam");
     if (!m) return cuopo_fail(CUOPO_EINVAL, "mlp_apply_adam: NULL argument");
     if (!(lr > 0) || !(grad_scale > 0)) return cuopo_fail(CUOPO_EINVAL, "mlp_apply_adam: lr and grad_scale must be > 0");
     cudaStream_t st = (cudaStream_t)stream;

@@ -363,6 +363,7 @@ static std::vector<unsigned char> build_tables(const cuopo_params &p, const floa
 extern "C" cuopo_status cuopo_plan_create(cuopo_plan **out, const cuopo_params *p,
                                           const float *w_host, const float *T_host, int precision)
 {
+    cuopo::Range range_("cuopo_plan_create");
     if (!out || !p) return cuopo_fail(CUOPO_EINVAL, "plan_create: NULL argument");
     *out = nullptr;
     if (p->n_eqs != 2 && p->n_eqs != 3) return cuopo_fail(CUOPO_EINVAL, "n_eqs must be 2 or 3");
@@ -537,6 +538,7 @@ static cuopo_status launch(cuopo_plan *pl, const LaunchArgs &a, int grid, void *
 
 extern "C" cuopo_status cuopo_crystal_pass(cuopo_plan *pl, void *Ap, void *As, void *Ai, void *stream)
 {
+    cuopo::Range range_("cuopo_crystal_pass");
     if (!pl || !Ap || !As || (pl->F == 3 && !Ai)) return cuopo_fail(CUOPO_EINVAL, "crystal_pass: NULL argument");
     LaunchArgs a = base_args(pl);
     a.pass_only = 1;
@@ -555,6 +557,7 @@ extern "C" cuopo_status cuopo_round_trips(cuopo_plan *pl, void *Ap, void *As, vo
                                           void *save_i, int save_first, int save_count, double *ps_hist,
                                           double tol, int *rt_done_dev, void *stream)
 {
+    cuopo::Range range_("cuopo_round_trips");
     if (!pl || !Ap || !As || (pl->F == 3 && !Ai)) return cuopo_fail(CUOPO_EINVAL, "round_trips: NULL field");
     if (rt_count < 0 || rt_begin < 0 || save_count < 0) return cuopo_fail(CUOPO_EINVAL, "round_trips: negative count");
     if (pl->p.regime == CUOPO_NS && (!pump || n_rt < 2))
@@ -880,6 +883,7 @@ static cuopo_status batch_build(cuopo_batch **out, const std::vector<cuopo_param
 extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params *base, const cuopo_instance *inst,
                                            int count, int precision)
 {
+    cuopo::Range range_("cuopo_batch_create");
     if (!out || !base || !inst || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create: bad argument");
     *out = nullptr;
     std::vector<cuopo_params> prm((size_t)count, *base);
@@ -899,6 +903,7 @@ extern "C" cuopo_status cuopo_batch_create(cuopo_batch **out, const cuopo_params
 extern "C" cuopo_status cuopo_batch_create_inputs(cuopo_batch **out, const cuopo_inputs *in, const uint64_t *seeds,
                                                   int count, int precision)
 {
+    cuopo::Range range_("cuopo_batch_create_inputs");
     if (!out || !in || count < 1) return cuopo_fail(CUOPO_EINVAL, "batch_create_inputs: bad argument");
     *out = nullptr;
     std::vector<cuopo_params> prm((size_t)count);
@@ -1010,6 +1015,7 @@ extern "C" cuopo_status cuopo_batch_reset(cuopo_batch *b, void *stream)
 extern "C" cuopo_status cuopo_batch_step(cuopo_batch *b, int chunk, int max_rt, double tol, int patience,
                                          void *stream)
 {
+    cuopo::Range range_("cuopo_batch_step");
     if (!b || chunk < 1 || max_rt < 1) return cuopo_fail(CUOPO_EINVAL, "batch_step: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = cudaEventRecord(b->fork, st);
@@ -1094,6 +1100,7 @@ extern "C" cuopo_status cuopo_batch_history(cuopo_batch *b, int i, double *ps, i
 extern "C" cuopo_status cuopo_autotune(const cuopo_params *base, int precision, int count, int n_rt, int *points_per_cta,
                                        int *cluster, double *ms)
 {
+    cuopo::Range range_("cuopo_autotune");
     if (!base || count < 1 || n_rt < 1) return cuopo_fail(CUOPO_EINVAL, "autotune: bad argument");
     const int F = base->n_eqs, N = base->n_t;
     std::vector<const KernelEntry *> cand;
