@@ -555,7 +555,7 @@ def run_cuopo(args):
             "cpu_baseline": cpu,
             "e2e": {"value": done_all / (e2e_ms * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(total * 8 / K), "d2h_bytes_per_step": int((total * 8 + len(insts) * 16) / K)},
-            "gpu_launches": K * len(set(nt_o.tolist())) + 0,
+            "gpu_launches": K * len(set(nt_o.tolist())),
             "clocks": clk,
             "validation_fp64": validation,
             "warm_start": warm_leg,
