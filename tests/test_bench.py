@@ -31,3 +31,16 @@ def test_reference_arm_imports_nothing_of_the_product():
                 assert not (node.module or "").startswith("cuopo_b200"), name
             elif isinstance(node, ast.Name):
                 assert node.id not in ("cu", "sweep", "shard"), (name, node.id)
+
+
+def test_flop_accounting_constants():
+    """The algorithmic work per round trip behind `roofline.achieved`: per
+    point and slice 10 F log2 N (forward and inverse transform of each field,
+    5 N log2 N each) + 328 (the 2-equation RK4 half steps) + 12 (linear
+    step), 600 for the 2^13 single CW OPO; per round trip 8 per point for the
+    cavity map and, with GDD, one more transform pair and phase per point."""
+    import bench
+    n = 8192
+    assert 10 * 2 * 13 + 328 + 12 == 600
+    assert bench.flops_per_instance_rt(n, 0.0) == bench.N_Z * n * 600 + 8 * n
+    assert bench.flops_per_instance_rt(n, 1e-4) == bench.N_Z * n * 600 + 8 * n + n * (10 * 13 + 6)
