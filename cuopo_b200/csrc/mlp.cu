@@ -1339,6 +1339,7 @@ extern "C" cuopo_status cuopo_fields_from_modes(const float *modes, int count, i
                                                 void *fields, void *stream)
 {
     if (!modes || !fields || count < 1) return cuopo_fail(CUOPO_EINVAL, "fields_from_modes: bad argument");
+    if (count > 65535) return cuopo_fail(CUOPO_EINVAL, "fields_from_modes: at most 65535 instances per call");
     if (n_modes < 16 || n_modes % 16 || n_modes > 1024 || n_modes > n_t || n_t < 16 || (n_t & (n_t - 1)))
         return cuopo_fail(CUOPO_EINVAL, "fields_from_modes: n_modes a multiple of 16 in [16, min(n_t, 1024)], "
                                         "n_t a power of 2");
@@ -1447,6 +1448,7 @@ extern "C" cuopo_status cuopo_fields_from_bands(const float *pred, int count, in
                                                 int *centres, void *stream)
 {
     if (!pred || !fields || count < 1) return cuopo_fail(CUOPO_EINVAL, "fields_from_bands: bad argument");
+    if (count > 65535) return cuopo_fail(CUOPO_EINVAL, "fields_from_bands: at most 65535 instances per call");
     if (n_t < 2 * BAND || (n_t & (n_t - 1)))
         return cuopo_fail(CUOPO_EINVAL, "fields_from_bands: n_t must be a power of 2 >= 256");
     dim3 grid((unsigned)((n_t + 255) / 256), (unsigned)count);

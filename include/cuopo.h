@@ -443,7 +443,8 @@ cuopo_status cuopo_gemm_bf16(const void *A, const void *B, float *C, int M, int 
  * modes_from_spectrum reads the modes back from the cuopo_fft_c2c sign -1
  * transform of a field (divided by n_t * scale) with the sign that makes
  * the largest mode's real part >= 0 (the 2-wave equations are invariant
- * under As -> -As).  Device arrays; fields are float pairs. */
+ * under As -> -As).  Device arrays; fields are float pairs;
+ * fields_from_modes takes at most 65535 instances per call. */
 cuopo_status cuopo_fields_from_modes(const float *modes, int count, int n_modes, int n_t, double scale, void *fields,
                                      void *stream);
 cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, int n_t, int n_modes, double scale, float *modes,
@@ -456,7 +457,8 @@ cuopo_status cuopo_modes_from_spectrum(const void *spec, int count, int n_t, int
  * |c_q| proportional to max(magnitude, 0), total power P (the means of the
  * copies; q0 rounded and clamped to [64, n_t/2 - 64]) and every mode of
  * phase Phi/2, so that each signal-idler pair c_q c_-q has the phase Phi.
- * centres (device, may be NULL) gets each instance's q0. */
+ * centres (device, may be NULL) gets each instance's q0.  At most 65535
+ * instances per call. */
 cuopo_status cuopo_fields_from_bands(const float *pred, int count, int n_t, double scale, void *fields, int *centres,
                                      void *stream);
 

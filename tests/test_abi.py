@@ -63,6 +63,9 @@ def test_new_entry_points_reject_bad_arguments_before_touching_the_gpu():
     # field synthesis: n_t not a power of 2 / too small, n_modes not a multiple of 16
     assert lib.cuopo_fields_from_bands(buf, 1, 100, 1.0, buf, None, None) == cu.EINVAL
     assert lib.cuopo_fields_from_modes(buf, 1, 20, 1024, 1.0, buf, None) == cu.EINVAL
+    # one grid row per instance: at most 65535 per call
+    assert lib.cuopo_fields_from_bands(buf, 65536, 1024, 1.0, buf, None, None) == cu.EINVAL
+    assert lib.cuopo_fields_from_modes(buf, 65536, 256, 1024, 1.0, buf, None) == cu.EINVAL
     assert lib.cuopo_modes_from_spectrum(buf, 1, 1024, 48, 1.0, buf, None) == cu.EINVAL
     # device set-up: NULL arrays, no instances
     assert lib.cuopo_derive_params_device(None, 4, None, None, None) == cu.EINVAL
